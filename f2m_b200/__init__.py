@@ -1,0 +1,324 @@
+"""f2m_b200: B200-native F2M (fractional 2-matching) solver.
+
+Python binding of the C ABI in include/f2m.h (libf2m_b200.so, built in-tree
+for sm_100a by f2m_b200/build.py).  The surface mirrors the reference's
+F2M.h graph API:
+
+    g = graph("file.tsp", 20)   # graph(std::string file, int E_max), F2M.h:181
+    graph_c(g)                  # graph_c(graph*), F2M.h:320
+    g.RUN()                     # graph::RUN(), F2M.h:175 -- writes the report files
+    g.X                         # graph::X, F2M.h:161: {edge id: x}
+
+plus batched and in-memory entry points (solve_batch, solve_points).  There is
+no CPU fallback: without the CUDA library or a device every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libf2m_b200.so")
+
+OK, ERR_INPUT, ERR_CAPACITY, ERR_NOT_CONVERGED, ERR_CUDA, ERR_NO_DEVICE = range(6)
+COST_REF_EUCLID, COST_NINT = 0, 1
+STATUS_NAMES = {0: "OK", 1: "ERR_INPUT", 2: "ERR_CAPACITY", 3: "ERR_NOT_CONVERGED",
+                4: "ERR_CUDA", 5: "ERR_NO_DEVICE"}
+
+
+class F2MError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"f2m status {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Params(ctypes.Structure):
+    """f2m_params: the reference's constants (defaults from f2m_default_params)."""
+    _fields_ = [
+        ("error_B", ctypes.c_double), ("error_B_comb", ctypes.c_double),
+        ("glob_K", ctypes.c_int32), ("glob_rounds", ctypes.c_int32),
+        ("glob_inner", ctypes.c_int32), ("glob_tol", ctypes.c_double),
+        ("factor0", ctypes.c_int32), ("factor_step", ctypes.c_int32),
+        ("factor_cap", ctypes.c_int32), ("max_rounds", ctypes.c_int32),
+        ("fix_rounds", ctypes.c_int32), ("fix_factor", ctypes.c_int32),
+        ("check_every", ctypes.c_int32), ("frozen_iters", ctypes.c_int32),
+        ("ef_thr", ctypes.c_double), ("ef_small_deg", ctypes.c_int32),
+        ("ef_min", ctypes.c_int32), ("comb_thr", ctypes.c_double),
+        ("shift0", ctypes.c_double), ("shift_max", ctypes.c_double),
+        ("max_iters", ctypes.c_int64), ("cost_mode", ctypes.c_int32),
+        ("threads", ctypes.c_int32),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int64), ("checks", ctypes.c_int32),
+        ("n_combs", ctypes.c_int32), ("irr_a", ctypes.c_int32), ("irr_b", ctypes.c_int32),
+        ("repair_steps", ctypes.c_int32), ("degree_violations", ctypes.c_int32),
+        ("max_grad", ctypes.c_double), ("d_min", ctypes.c_double),
+        ("dual_value", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Work(ctypes.Structure):
+    _fields_ = [("node_iters", ctypes.c_int64), ("slot_iters", ctypes.c_int64),
+                ("slots", ctypes.c_int64), ("points", ctypes.c_int64)]
+
+
+class BatchOut(ctypes.Structure):
+    _fields_ = [("lp", ctypes.c_void_p), ("status", ctypes.c_void_p),
+                ("n_nodes", ctypes.c_void_p), ("n_edges", ctypes.c_void_p),
+                ("n_combs", ctypes.c_void_p), ("max_rank", ctypes.c_void_p),
+                ("iterations", ctypes.c_void_p)]
+
+
+# Every symbol include/f2m.h declares.
+EXPORTS = [
+    "f2m_default_params", "f2m_create", "f2m_destroy", "f2m_last_error", "f2m_kernel_launches",
+    "f2m_solve_batch", "f2m_solve_batch_device", "f2m_sync", "f2m_solve_points",
+    "f2m_solve_file", "f2m_result_free", "f2m_result_status", "f2m_result_n_nodes",
+    "f2m_result_n_edges", "f2m_result_lp", "f2m_result_max_rank", "f2m_result_seconds",
+    "f2m_result_edges", "f2m_result_nodes", "f2m_result_stats", "f2m_phase_times",
+]
+
+_lib = None
+
+
+def lib():
+    """Load libf2m_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise F2MError(ERR_NO_DEVICE, f"{LIB_PATH} is missing: run f2m_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, i64, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+        P = ctypes.POINTER
+        L.f2m_default_params.argtypes = [P(Params)]
+        L.f2m_create.argtypes = [P(vp), ctypes.c_int]
+        L.f2m_destroy.argtypes = [vp]
+        L.f2m_last_error.argtypes = [vp]
+        L.f2m_last_error.restype = ctypes.c_char_p
+        L.f2m_kernel_launches.argtypes = [vp]
+        L.f2m_kernel_launches.restype = i64
+        L.f2m_sync.argtypes = [vp]
+        L.f2m_solve_batch.argtypes = [vp, i32, vp, vp, vp, i32, P(Params), P(BatchOut)]
+        L.f2m_solve_batch_device.argtypes = [vp, i32, vp, vp, vp, vp, i32, P(Params), P(BatchOut)]
+        L.f2m_solve_points.argtypes = [vp, vp, vp, vp, i32, i32, P(Params), P(vp)]
+        L.f2m_solve_file.argtypes = [vp, ctypes.c_char_p, i32, P(Params), i32, P(vp)]
+        L.f2m_result_free.argtypes = [vp]
+        for name in ("f2m_result_status", "f2m_result_n_nodes", "f2m_result_n_edges",
+                     "f2m_result_max_rank"):
+            getattr(L, name).argtypes = [vp]
+            getattr(L, name).restype = i32
+        for name in ("f2m_result_lp", "f2m_result_seconds"):
+            getattr(L, name).argtypes = [vp]
+            getattr(L, name).restype = dbl
+        L.f2m_result_edges.argtypes = [vp] * 8
+        L.f2m_result_nodes.argtypes = [vp] * 3
+        L.f2m_result_stats.argtypes = [vp, P(Stats)]
+        L.f2m_phase_times.argtypes = [vp, vp, P(Work)]
+        _lib = L
+    return _lib
+
+
+def default_params(**overrides):
+    p = Params()
+    lib().f2m_default_params(ctypes.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """One f2m context (one CUDA stream on one device)."""
+
+    def __init__(self, device=0):
+        self._h = ctypes.c_void_p()
+        s = lib().f2m_create(ctypes.byref(self._h), device)
+        if s != OK:
+            raise F2MError(s, "no usable CUDA device")
+
+    def close(self):
+        if self._h:
+            lib().f2m_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def last_error(self):
+        return lib().f2m_last_error(self._h).decode()
+
+    def kernel_launches(self):
+        return lib().f2m_kernel_launches(self._h)
+
+    def _check(self, s):
+        if s not in (OK, ERR_NOT_CONVERGED):
+            raise F2MError(s, self.last_error())
+        return s
+
+    # -- batched ----------------------------------------------------------
+    def solve_batch(self, offs, x, y, top_k, params=None, details=False):
+        """Solve independent instances; offs[b]..offs[b+1] index x/y (host arrays).
+
+        Returns (lp, status) or, with details=True, a dict of all per-instance
+        outputs."""
+        offs = np.ascontiguousarray(offs, np.int64)
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        n = len(offs) - 1
+        lp = np.zeros(n, np.float64)
+        st = np.zeros(n, np.int32)
+        o = BatchOut(lp=lp.ctypes.data, status=st.ctypes.data)
+        extra = {}
+        if details:
+            for k, dt in (("n_nodes", np.int32), ("n_edges", np.int32), ("n_combs", np.int32),
+                          ("max_rank", np.int32), ("iterations", np.int64)):
+                extra[k] = np.zeros(n, dt)
+                setattr(o, k, extra[k].ctypes.data)
+        p = params if params is not None else default_params()
+        self._check(lib().f2m_solve_batch(self._h, n, _ptr(offs), _ptr(x), _ptr(y), top_k,
+                                          ctypes.byref(p), ctypes.byref(o)))
+        if details:
+            extra.update(lp=lp, status=st)
+            return extra
+        return lp, st
+
+    def solve_batch_device(self, h_offs, d_offs, d_x, d_y, top_k, d_lp, d_status, params=None,
+                           d_iterations=None):
+        """Device-resident batch: d_* are device addresses (ints); outputs too."""
+        h_offs = np.ascontiguousarray(h_offs, np.int64)
+        n = len(h_offs) - 1
+        o = BatchOut(lp=d_lp, status=d_status, iterations=d_iterations)
+        p = params if params is not None else default_params()
+        self._check(lib().f2m_solve_batch_device(self._h, n, _ptr(h_offs), ctypes.c_void_p(d_offs),
+                                                 ctypes.c_void_p(d_x), ctypes.c_void_p(d_y), top_k,
+                                                 ctypes.byref(p), ctypes.byref(o)))
+
+    def sync(self):
+        self._check(lib().f2m_sync(self._h))
+
+    def phase_times(self):
+        """(ms per phase [prep, knn, graph, solve], work counters) of the last batch."""
+        ms = np.zeros(4, np.float32)
+        w = Work()
+        self._check(lib().f2m_phase_times(self._h, _ptr(ms), ctypes.byref(w)))
+        return ms, {k: getattr(w, k) for k, _ in Work._fields_}
+
+    # -- single instance ----------------------------------------------------
+    def solve_points(self, x, y, top_k, labels=None, params=None):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        lab = None if labels is None else np.ascontiguousarray(labels, np.int32)
+        h = ctypes.c_void_p()
+        p = params if params is not None else default_params()
+        s = lib().f2m_solve_points(self._h, _ptr(x), _ptr(y), _ptr(lab), len(x), top_k,
+                                   ctypes.byref(p), ctypes.byref(h))
+        return self._result(s, h)
+
+    def solve_file(self, path, top_k, params=None, write_files=False):
+        h = ctypes.c_void_p()
+        p = params if params is not None else default_params()
+        s = lib().f2m_solve_file(self._h, os.fsencode(path), top_k, ctypes.byref(p),
+                                 1 if write_files else 0, ctypes.byref(h))
+        return self._result(s, h)
+
+    def _result(self, s, h):
+        if not h:
+            raise F2MError(s, self.last_error())
+        try:
+            return Result(h)
+        finally:
+            lib().f2m_result_free(h)
+
+
+class Result:
+    """Host copy of one solved instance (graph + potentials + primal)."""
+
+    def __init__(self, h):
+        L = lib()
+        self.status = L.f2m_result_status(h)
+        self.n_nodes = L.f2m_result_n_nodes(h)
+        self.n_edges = L.f2m_result_n_edges(h)
+        self.lp = L.f2m_result_lp(h)
+        self.max_rank = L.f2m_result_max_rank(h)
+        self.seconds = L.f2m_result_seconds(h)
+        ne, nv = self.n_edges, self.n_nodes
+        self.v1 = np.zeros(ne, np.int32)
+        self.v2 = np.zeros(ne, np.int32)
+        self.lab1 = np.zeros(ne, np.int32)
+        self.lab2 = np.zeros(ne, np.int32)
+        self.Do = np.zeros(ne, np.float64)
+        self.D = np.zeros(ne, np.float64)
+        self.x = np.zeros(ne, np.float64)
+        if ne:
+            L.f2m_result_edges(h, *(_ptr(a) for a in (self.v1, self.v2, self.lab1, self.lab2,
+                                                      self.Do, self.D, self.x)))
+        self.label = np.zeros(nv, np.int32)
+        self.F = np.zeros(nv, np.float64)
+        if nv:
+            L.f2m_result_nodes(h, _ptr(self.label), _ptr(self.F))
+        st = Stats()
+        L.f2m_result_stats(h, ctypes.byref(st))
+        self.stats = st.as_dict()
+
+    def edge_set(self):
+        a = np.minimum(self.lab1, self.lab2)
+        b = np.maximum(self.lab1, self.lab2)
+        return set(zip(a.tolist(), b.tolist()))
+
+    @property
+    def X(self):
+        """graph::X: {edge id: x} for edges in the primal solution."""
+        nz = np.nonzero(self.x)[0]
+        return {int(e): float(self.x[e]) for e in nz}
+
+
+# ---------------------------------------------------------------------------
+# The reference's graph API (F2M.h) over the context
+# ---------------------------------------------------------------------------
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class graph:
+    """graph(file, E_max) -- F2M.h:181.  RUN() solves and writes the report files."""
+
+    def __init__(self, file, E_max, params=None, ctx=None):
+        self.file = file
+        self.E_max = int(E_max)
+        self.params = params
+        self.ctx = ctx or default_context()
+        self.result = None
+        self.X = {}
+
+    def RUN(self):
+        """graph::RUN (graph_cuda.cu:47-155)."""
+        self.result = self.ctx.solve_file(self.file, self.E_max, self.params, write_files=True)
+        self.X = self.result.X
+        return self.result
+
+
+def graph_c(g):
+    """graph_c(graph*) -- F2M.h:320.  Device set-up happens inside RUN()."""
+    return g

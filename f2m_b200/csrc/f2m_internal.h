@@ -1,0 +1,123 @@
+// Internal declarations shared by the CUDA kernels (f2m_kernels.cu) and the
+// host runtime (f2m_runtime.cpp).  Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/f2m.h"
+
+namespace f2m {
+
+// Internal status: the instance needs the host comb solve (Ax=b) because at
+// least one comb violates 2A+B=4 (comb_thread.cpp:180-195).
+constexpr int32_t kNeedsHost = 100;
+
+// One CSR slot as the solver reads it: normalised cost D and neighbour id.
+// `aux` holds the slot's original position in its node's list (the edge's
+// rankDo at that endpoint, node.cpp:18).
+struct __align__(16) Slot {
+    double D;
+    int32_t nbr;
+    int32_t aux;
+};
+
+// Device-side constants of one solve call (the reference's constants).
+struct DevParams {
+    double error_B, porog, glob_tol, ef_thr, comb_thr;
+    int32_t glob_K, glob_rounds, glob_inner;
+    int32_t factor0, factor_step, factor_cap, max_rounds;
+    int32_t fix_rounds, fix_factor, check_every, frozen_iters;
+    int32_t ef_small_deg, ef_min;
+    int64_t max_iters;
+};
+
+// Pointers of one batched call.  Node g of instance b lives at index
+// offs[b] + local id; slots of node g are [row[g], row[g+1]).
+struct Batch {
+    int32_t n_inst;
+    int32_t N;              // neighbours selected per node (top_k, E_max)
+    int32_t N_cut;          // top_k of the cut-off pass (FXY.hpp:77-78); normally N
+    int32_t n_total;        // points over all instances (before de-duplication)
+    const int64_t* offs;    // [n_inst+1]
+    const double* X_in;     // raw coordinates [n_total]
+    const double* Y_in;
+    const int32_t* K_in;    // labels or nullptr (then label = local index + 1)
+    double2* Pr;            // rounded, not compacted [n_total]
+    double2* P;             // rounded, de-duplicated, compacted [n_total]
+    int32_t* K;             // labels of P [n_total]
+    int32_t* dup_of;        // [n_total] input index -> local id of the kept copy, -1 if kept
+    int32_t* Vn;            // [n_inst]
+    double* spn;            // size_per_node [n_inst]
+    unsigned long long* dmin_bits;  // [n_inst] min edge cost (as ordered bits)
+    int32_t* status;        // [n_inst]
+    // kNN
+    double* cut;            // [n_total]
+    int32_t* stat;          // [n_total]
+    int32_t* ntop;          // [n_total]
+    int32_t* top_nbr;       // [n_total*N]
+    double* top_cost;       // [n_total*N]
+    int32_t* top_em;        // [n_total*N]
+    int32_t* top_oth;       // [n_total*N]
+    // graph
+    int32_t* rev;           // [n_total]
+    int32_t* cursor;        // [n_total]
+    int64_t* row;           // [n_total+1]
+    int32_t* s_nbr;         // [S]
+    double* s_cost;         // [S] raw cost Do
+    int32_t* s_em;          // [S]
+    int32_t* s_oth;         // [S]
+    Slot* slot;             // [S]
+    uint16_t* perm;         // [S] per-node list order (local positions)
+    int32_t* mirror;        // [S] position of the same edge in the neighbour's list
+    Slot* ef;               // [S] active-set arena (update_EF copies)
+    uint8_t* xcode;         // [S] 0, 1 (= 1/2), 2 (= 1)
+    int64_t S_cap;
+    // per-node state kept between the solve and the host comb check
+    double* F;              // [n_total] potentials
+    int32_t* efcnt;         // [n_total] EF list length (cuda_EF_NodesStat)
+    int32_t* ccnt;          // [n_total] comb prefix length (cuda_COMB_NodesStat)
+    const double* shift;    // [n_total] repair shift per node (k_refit input; 0 = none)
+    // per-instance results
+    double* lp;
+    int32_t* n_edges;
+    int32_t* n_combs;
+    int32_t* n_irr;
+    int32_t* max_rank;
+    int32_t* deg_viol;
+    int64_t* iters;
+    int64_t* work_nodes;    // sum over Jacobi iterations of V
+    int64_t* work_slots;    // sum over Jacobi iterations of active slots
+    int32_t* checks;
+    double* max_grad;
+    double* dual;
+    // work lists
+    const int32_t* chunk_inst;  // node-parallel work items
+    const int32_t* chunk_start;
+    int32_t n_chunks;
+    const int32_t* order;       // instances to run, largest first
+    int32_t n_items;            // entries of `order`
+    int32_t* queue;             // persistent-kernel work counter
+};
+
+// Host-side launchers (f2m_kernels.cu).
+cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches);
+cudaError_t launch_knn(const Batch& B, cudaStream_t s, int64_t* launches);
+cudaError_t launch_graph(const Batch& B, int64_t* deg_scratch, int64_t* scan_scratch,
+                         cudaStream_t s, int64_t* launches);
+cudaError_t launch_solve(const Batch& B, const DevParams& P, int32_t v_max, int threads,
+                         cudaStream_t s, int64_t* launches);
+// Repair step for the instances listed in B.order[0..B.n_items): F += shift,
+// frozen iterations, run_fix, comb partition (graph_cuda_comb.hpp:542-574).
+cudaError_t launch_refit(const Batch& B, const DevParams& P, int32_t v_max, int threads,
+                         cudaStream_t s, int64_t* launches);
+cudaError_t launch_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* scratch,
+                        cudaStream_t s, int64_t* launches);
+int64_t scan_scratch_elems(int64_t n);
+int solve_blocks_per_sm(int threads, size_t smem);
+size_t solve_smem_bytes(int32_t v_max);
+int32_t solve_max_nodes();
+
+}  // namespace f2m

@@ -1,0 +1,1106 @@
+// f2m_b200 CUDA kernels for sm_100a.
+//
+// Pipeline of one batched call (one CTA = one instance unless noted):
+//   k_prep      1e-3 rounding, de-duplication, compaction, bbox   (FXY.hpp:231-309)
+//   k_cutoff    per-node ring cut-off radius (stat pass)          (FXY.hpp:441-534)
+//   k_select    per-node first-N neighbours by (d, emitter, partner)
+//                                                    (FXY.hpp:347-437 + graph_tour.hpp:28-90)
+//   k_graph_*   union-of-kNN CSR in edge order, mirror slots, D = Do/d_min
+//                                     (graph_tour.hpp:28-98, graph_cuda_init.hpp:3-96)
+//   k_solve     persistent CTA per instance: the whole descent schedule
+//               (graph_cuda.cu:163-430), partitions (graph_cuda_partition.hpp),
+//               comb extraction (graph_cuda_comb.hpp:201-475), the comb check
+//               (comb_thread.cpp:180-195) and the primal value
+//               (graph_cuda.cu:135-147, graph_tour.hpp:165-184).
+//
+// All solver arithmetic is FP64 and evaluates exactly the reference's
+// expressions, so a node's potential F follows the reference's trajectory
+// bit for bit (given the same node ids).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "f2m_internal.h"
+
+namespace f2m {
+
+constexpr int kT = 256;       // width of the node-parallel kernels
+constexpr int kTile = 1024;   // points per shared-memory tile (16 KB)
+constexpr int kMaxPasses = 64;
+
+/* ------------------------------------------------------------------ */
+/* block-level helpers                                                  */
+/* ------------------------------------------------------------------ */
+template <int T>
+__device__ __forceinline__ double block_max(double x, double* sred) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    if (lane == 0) sred[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        x = (lane < T / 32) ? sred[lane] : -INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0) sred[0] = x;
+    }
+    __syncthreads();
+    double r = sred[0];
+    __syncthreads();
+    return r;
+}
+template <int T>
+__device__ __forceinline__ double block_min(double x, double* sred) {
+    return -block_max<T>(-x, sred);
+}
+template <int T>
+__device__ __forceinline__ double block_sum(double x, double* sred) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sred[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        x = (lane < T / 32) ? sred[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sred[0] = x;
+    }
+    __syncthreads();
+    double r = sred[0];
+    __syncthreads();
+    return r;
+}
+template <int T>
+__device__ __forceinline__ long long block_sum_ll(long long x, long long* sred) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sred[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        x = (lane < T / 32) ? sred[lane] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sred[0] = x;
+    }
+    __syncthreads();
+    long long r = sred[0];
+    __syncthreads();
+    return r;
+}
+template <int T>
+__device__ __forceinline__ long long block_max_ll(long long x, long long* sred) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = max(x, (long long)__shfl_xor_sync(0xffffffffu, x, o));
+    if (lane == 0) sred[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        x = (lane < T / 32) ? sred[lane] : LLONG_MIN;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = max(x, (long long)__shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0) sred[0] = x;
+    }
+    __syncthreads();
+    long long r = sred[0];
+    __syncthreads();
+    return r;
+}
+// Exclusive scan of one int per thread in thread order; *total = block sum.
+// swarp needs T/32 + 1 ints.
+template <int T>
+__device__ __forceinline__ int block_excl_scan(int x, int* swarp, int* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) swarp[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int s = (lane < T / 32) ? swarp[lane] : 0;
+        int incs = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, incs, o);
+            if (lane >= o) incs += y;
+        }
+        if (lane < T / 32) swarp[lane] = incs - s;
+        if (lane == T / 32 - 1) swarp[T / 32] = incs;
+    }
+    __syncthreads();
+    int r = swarp[w] + inc - x;
+    *total = swarp[T / 32];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ double round3(double x) {
+    double r = round(x * 1000.0);  // std::round: half away from zero, as FXY.hpp:252
+    return r / 1000.0;
+}
+
+/* ------------------------------------------------------------------ */
+/* k_prep: rounding, de-duplication, compaction, bbox (FXY.hpp:231-309)  */
+/* ------------------------------------------------------------------ */
+__global__ void __launch_bounds__(kT) k_prep(Batch B) {
+    const int b = blockIdx.x;
+    const int64_t base = B.offs[b];
+    const int n = (int)(B.offs[b + 1] - base);
+    __shared__ double2 tile[kTile];
+    __shared__ int swarp[kT / 32 + 1];
+    __shared__ int s_carry;
+    __shared__ double sred[kT / 32];
+
+    for (int i = threadIdx.x; i < n; i += kT) {
+        B.Pr[base + i] = make_double2(round3(B.X_in[base + i]), round3(B.Y_in[base + i]));
+        B.dup_of[base + i] = -1;
+    }
+    __syncthreads();
+    // a point is dropped if an earlier point has identical rounded
+    // coordinates; it maps to the first such point (FXY.hpp:260-265)
+    for (int t0 = 0; t0 < n; t0 += kTile) {
+        const int cnt = min(kTile, n - t0);
+        for (int k = threadIdx.x; k < cnt; k += kT) tile[k] = B.Pr[base + t0 + k];
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += kT) {
+            if (i <= t0 || B.dup_of[base + i] >= 0) continue;
+            const double2 p = B.Pr[base + i];
+            const int jmax = min(cnt, i - t0);
+            for (int k = 0; k < jmax; ++k)
+                if (tile[k].x == p.x && tile[k].y == p.y) { B.dup_of[base + i] = t0 + k; break; }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int r = 0; r < n; r += kT) {
+        const int i = r + threadIdx.x;
+        const int keep = (i < n && B.dup_of[base + i] < 0) ? 1 : 0;
+        int tot;
+        const int ex = block_excl_scan<kT>(keep, swarp, &tot);
+        if (keep) {
+            const int id = s_carry + ex;
+            B.P[base + id] = B.Pr[base + i];
+            B.K[base + id] = B.K_in ? B.K_in[base + i] : i + 1;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += tot;
+        __syncthreads();
+    }
+    const int V = s_carry;
+    double mnx = INFINITY, mxx = -INFINITY, mny = INFINITY, mxy = -INFINITY;
+    for (int i = threadIdx.x; i < V; i += kT) {
+        const double2 p = B.P[base + i];
+        mnx = fmin(mnx, p.x); mxx = fmax(mxx, p.x);
+        mny = fmin(mny, p.y); mxy = fmax(mxy, p.y);
+    }
+    mnx = block_min<kT>(mnx, sred);
+    mxx = block_max<kT>(mxx, sred);
+    mny = block_min<kT>(mny, sred);
+    mxy = block_max<kT>(mxy, sred);
+    if (threadIdx.x == 0) {
+        // FXY.hpp:305-306 with the area widened to 64 bits; a zero x-span
+        // falls back to the y-span (the reference never terminates there)
+        const double sx = mxx - mnx, sy = mxy - mny;
+        int st = F2M_OK;
+        double spn = 0.0;
+        if (V < 4 || !(sx * sx < 9.0e18) || !(sy * sy < 9.0e18)) {
+            st = F2M_ERR_INPUT;
+        } else {
+            long long area = (long long)(sx * sx);
+            if (area == 0) area = (long long)(sy * sy);
+            if (area == 0) st = F2M_ERR_INPUT;
+            else spn = sqrt((double)area / (double)V);
+        }
+        B.Vn[b] = V;
+        B.spn[b] = spn;
+        B.status[b] = st;
+        B.dmin_bits[b] = 0x7ff0000000000000ull;  // +inf
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* k_cutoff: ring counting with radius doubling (FXY.hpp:441-534)       */
+/* ------------------------------------------------------------------ */
+__global__ void __launch_bounds__(kT) k_cutoff(Batch B) {
+    const int c = blockIdx.x;
+    const int b = B.chunk_inst[c];
+    if (B.status[b] != F2M_OK) return;
+    const int V = B.Vn[b];
+    const int i0 = B.chunk_start[c];
+    if (i0 >= V) return;
+    const int64_t base = B.offs[b];
+    const int i = i0 + threadIdx.x;
+    const bool active = i < V;
+    const int N = min(B.N_cut, V - 1);  // FXY.hpp:77
+    const double s = 2.0 * B.spn[b];  // FXY.hpp:78
+    const double2 me = active ? B.P[base + i] : make_double2(0.0, 0.0);
+    __shared__ double2 tile[kTile];
+
+    int L = 0, st = 0, passes = 0;
+    double cut = 0.0;
+    bool need = active;
+    while (__syncthreads_or(need)) {
+        const double sL = s * (double)L;
+        double lim[5], lo[5], hi[5];
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+            lim[j] = fma(s, (double)j, sL);  // nvcc's contraction of s*j + s*L
+            const double l2 = lim[j] * lim[j];
+            lo[j] = l2 * (1.0 - 0x1p-40);
+            hi[j] = l2 * (1.0 + 0x1p-40);
+        }
+        int cnt1 = 0, cnt2 = 0, cnt3 = 0, cnt4 = 0;
+        for (int t0 = 0; t0 < V; t0 += kTile) {
+            const int nt = min(kTile, V - t0);
+            __syncthreads();
+            for (int k = threadIdx.x; k < nt; k += kT) tile[k] = B.P[base + t0 + k];
+            __syncthreads();
+            if (need) {
+                for (int k = 0; k < nt; ++k) {
+                    const double dX = fabs(me.x - tile[k].x), dY = fabs(me.y - tile[k].y);
+                    const double q = fma(dY, dY, dX * dX);
+                    if (q >= hi[4] || t0 + k == i) continue;
+                    // counts[j] = #{ sqrt(q) < lim[j] } (FXY.hpp:479-482); the
+                    // square root is taken only inside the rounding band
+                    double d = -1.0;
+                    bool in;
+#define F2M_RING(J, CNT)                                             \
+    if (q < lo[J]) in = true;                                        \
+    else if (q >= hi[J]) in = false;                                 \
+    else { if (d < 0.0) d = sqrt(q); in = d < lim[J]; }              \
+    if (!in) continue;                                               \
+    CNT++;
+                    F2M_RING(4, cnt4)
+                    F2M_RING(3, cnt3)
+                    F2M_RING(2, cnt2)
+                    F2M_RING(1, cnt1)
+#undef F2M_RING
+                }
+            }
+        }
+        if (need) {
+            const int cnts[5] = {0, cnt1, cnt2, cnt3, cnt4};
+            st = 0;
+            cut = lim[0];
+#pragma unroll
+            for (int j = 1; j < 5; ++j) {  // FXY.hpp:486-502
+                st = cnts[j];
+                cut = lim[j];
+                if (cnts[j] > N) break;
+            }
+            if (st >= N) need = false;
+            L = (L == 0) ? 5 : 2 * L;
+            if (++passes >= kMaxPasses) need = false;
+        }
+    }
+    if (active) {
+        B.cut[base + i] = cut;
+        B.stat[base + i] = st;
+        if (st < N) B.status[b] = F2M_ERR_CAPACITY;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* k_select: first-N incident candidates of each node                   */
+/* ------------------------------------------------------------------ */
+// Key of the pair (i,j) at distance d in the reference's global candidate
+// order: thrust::sort by d, ties in emission order, where the pair a<b is
+// emitted by a when d <= cut[a] and by b otherwise (FXY.hpp:388-432).
+__device__ __forceinline__ bool key_less(double d1, int e1, int o1, double d2, int e2, int o2) {
+    if (d1 != d2) return d1 < d2;
+    if (e1 != e2) return e1 < e2;
+    return o1 < o2;
+}
+
+template <int NMAX>
+__global__ void __launch_bounds__(kT) k_select(Batch B) {
+    const int c = blockIdx.x;
+    const int b = B.chunk_inst[c];
+    if (B.status[b] != F2M_OK) return;
+    const int V = B.Vn[b];
+    const int i0 = B.chunk_start[c];
+    if (i0 >= V) return;
+    const int64_t base = B.offs[b];
+    const int i = i0 + threadIdx.x;
+    const bool active = i < V;
+    const int N = min(B.N, V - 1);
+    const double2 me = active ? B.P[base + i] : make_double2(0.0, 0.0);
+    __shared__ double2 tile[kTile];
+
+    double kd[NMAX];
+    int ke[NMAX], ko[NMAX];
+    int cnt = 0;
+    double worst_hi = INFINITY;
+    for (int t0 = 0; t0 < V; t0 += kTile) {
+        const int nt = min(kTile, V - t0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < nt; k += kT) tile[k] = B.P[base + t0 + k];
+        __syncthreads();
+        if (!active) continue;
+        for (int k = 0; k < nt; ++k) {
+            const int j = t0 + k;
+            const double dX = fabs(me.x - tile[k].x), dY = fabs(me.y - tile[k].y);
+            const double q = fma(dY, dY, dX * dX);
+            if (q > worst_hi || j == i) continue;
+            const double d = sqrt(q);
+            int em = i, oth = j;
+            if (j < i && d <= B.cut[base + j]) { em = j; oth = i; }
+            int pos;
+            if (cnt == N) {
+                if (!key_less(d, em, oth, kd[N - 1], ke[N - 1], ko[N - 1])) continue;
+                pos = N - 1;
+            } else {
+                pos = cnt++;
+            }
+            while (pos > 0 && key_less(d, em, oth, kd[pos - 1], ke[pos - 1], ko[pos - 1])) {
+                kd[pos] = kd[pos - 1]; ke[pos] = ke[pos - 1]; ko[pos] = ko[pos - 1];
+                --pos;
+            }
+            kd[pos] = d; ke[pos] = em; ko[pos] = oth;
+            if (cnt == N) worst_hi = kd[N - 1] * kd[N - 1] * (1.0 + 0x1p-40);
+        }
+    }
+    if (active) {
+        const int64_t o = (base + i) * (int64_t)B.N;
+        B.ntop[base + i] = cnt;
+        for (int k = 0; k < cnt; ++k) {
+            B.top_nbr[o + k] = (ke[k] == i) ? ko[k] : ke[k];
+            B.top_cost[o + k] = kd[k];
+            B.top_em[o + k] = ke[k];
+            B.top_oth[o + k] = ko[k];
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* graph build: union of the per-node lists (graph_tour.hpp:28-98)      */
+/* ------------------------------------------------------------------ */
+__device__ __forceinline__ bool in_top(const Batch& B, int64_t base, int j, int i) {
+    const int64_t o = (base + j) * (int64_t)B.N;
+    const int n = B.ntop[base + j];
+    for (int m = 0; m < n; ++m)
+        if (B.top_nbr[o + m] == i) return true;
+    return false;
+}
+
+__global__ void __launch_bounds__(kT) k_graph_rev(Batch B) {
+    const int c = blockIdx.x;
+    const int b = B.chunk_inst[c];
+    if (B.status[b] != F2M_OK) return;
+    const int V = B.Vn[b];
+    const int i = B.chunk_start[c] + threadIdx.x;
+    if (i >= V) return;
+    const int64_t base = B.offs[b];
+    const int64_t o = (base + i) * (int64_t)B.N;
+    const int nt = B.ntop[base + i];
+    for (int k = 0; k < nt; ++k) {
+        const int j = B.top_nbr[o + k];
+        if (!in_top(B, base, j, i)) atomicAdd(&B.rev[base + j], 1);
+    }
+    // d_min over kept edges (graph_tour.hpp:70): the smallest cost of a
+    // node's list is its first entry; positive doubles order like their bits
+    if (nt > 0) atomicMin(&B.dmin_bits[b], (unsigned long long)__double_as_longlong(B.top_cost[o]));
+}
+
+// degree per input position (0 for dropped duplicates and padding)
+__global__ void __launch_bounds__(kT) k_graph_deg(Batch B, int64_t* deg) {
+    const int c = blockIdx.x;
+    const int b = B.chunk_inst[c];
+    const int i = B.chunk_start[c] + threadIdx.x;
+    const int64_t base = B.offs[b];
+    const int n = (int)(B.offs[b + 1] - base);
+    if (i >= n) return;
+    int64_t d = 0;
+    if (B.status[b] == F2M_OK && i < B.Vn[b]) d = B.ntop[base + i] + B.rev[base + i];
+    deg[base + i] = d;
+}
+
+__global__ void __launch_bounds__(kT) k_graph_fill(Batch B) {
+    const int c = blockIdx.x;
+    const int b = B.chunk_inst[c];
+    if (B.status[b] != F2M_OK) return;
+    const int V = B.Vn[b];
+    const int i = B.chunk_start[c] + threadIdx.x;
+    if (i >= V) return;
+    const int64_t base = B.offs[b];
+    const int64_t o = (base + i) * (int64_t)B.N;
+    const int nt = B.ntop[base + i];
+    const int64_t r = B.row[base + i];
+    for (int k = 0; k < nt; ++k) {
+        const int j = B.top_nbr[o + k];
+        const double cost = B.top_cost[o + k];
+        const int em = B.top_em[o + k], oth = B.top_oth[o + k];
+        B.s_nbr[r + k] = j; B.s_cost[r + k] = cost; B.s_em[r + k] = em; B.s_oth[r + k] = oth;
+        if (!in_top(B, base, j, i)) {
+            const int p = atomicAdd(&B.cursor[base + j], 1);
+            const int64_t s2 = B.row[base + j] + B.ntop[base + j] + p;
+            B.s_nbr[s2] = i; B.s_cost[s2] = cost; B.s_em[s2] = em; B.s_oth[s2] = oth;
+        }
+    }
+}
+
+// Sort each node's slots by the global edge order; the result is the
+// reference's per-node list (edges pushed in edge-id order, graph_tour.hpp:87-88).
+__global__ void __launch_bounds__(kT) k_graph_sort(Batch B) {
+    const int c = blockIdx.x;
+    const int b = B.chunk_inst[c];
+    if (B.status[b] != F2M_OK) return;
+    const int V = B.Vn[b];
+    const int i = B.chunk_start[c] + threadIdx.x;
+    if (i >= V) return;
+    const int64_t base = B.offs[b];
+    const int64_t r0 = B.row[base + i], r1 = B.row[base + i + 1];
+    if (r1 - r0 > 65535) { B.status[b] = F2M_ERR_CAPACITY; return; }
+    for (int64_t a = r0 + 1; a < r1; ++a) {
+        const double kd = B.s_cost[a];
+        const int ke = B.s_em[a], ko = B.s_oth[a], kn = B.s_nbr[a];
+        int64_t p = a;
+        while (p > r0 && key_less(kd, ke, ko, B.s_cost[p - 1], B.s_em[p - 1], B.s_oth[p - 1])) {
+            B.s_cost[p] = B.s_cost[p - 1]; B.s_em[p] = B.s_em[p - 1];
+            B.s_oth[p] = B.s_oth[p - 1]; B.s_nbr[p] = B.s_nbr[p - 1];
+            --p;
+        }
+        B.s_cost[p] = kd; B.s_em[p] = ke; B.s_oth[p] = ko; B.s_nbr[p] = kn;
+    }
+    const double dmin = __longlong_as_double((long long)B.dmin_bits[b]);
+    for (int64_t a = r0; a < r1; ++a) {
+        Slot s;
+        s.D = B.s_cost[a] / dmin;  // F2M.h:101
+        s.nbr = B.s_nbr[a];
+        s.aux = (int32_t)(a - r0);
+        B.slot[a] = s;
+        B.perm[a] = (uint16_t)(a - r0);
+    }
+}
+
+__global__ void __launch_bounds__(kT) k_graph_mirror(Batch B) {
+    const int c = blockIdx.x;
+    const int b = B.chunk_inst[c];
+    if (B.status[b] != F2M_OK) return;
+    const int V = B.Vn[b];
+    const int i = B.chunk_start[c] + threadIdx.x;
+    if (i >= V) return;
+    const int64_t base = B.offs[b];
+    const int64_t r0 = B.row[base + i], r1 = B.row[base + i + 1];
+    for (int64_t a = r0; a < r1; ++a) {
+        const int j = B.s_nbr[a];
+        const int64_t q0 = B.row[base + j], q1 = B.row[base + j + 1];
+        int m = -1;
+        for (int64_t q = q0; q < q1; ++q)
+            if (B.s_nbr[q] == i) { m = (int)(q - q0); break; }
+        B.mirror[a] = m;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* exclusive scan of int64 (row offsets)                                */
+/* ------------------------------------------------------------------ */
+constexpr int kScanPer = 4;
+constexpr int kScanBlock = kT * kScanPer;
+
+__global__ void __launch_bounds__(kT) k_scan_local(const int64_t* in, int64_t* out, int64_t n,
+                                                   int64_t* sums) {
+    __shared__ long long swarp[kT / 32 + 1];
+    const int64_t o = (int64_t)blockIdx.x * kScanBlock + threadIdx.x * kScanPer;
+    long long v[kScanPer];
+    long long tsum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        v[k] = (o + k < n) ? in[o + k] : 0;
+        tsum += v[k];
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long inc = tsum;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        long long y = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += y;
+    }
+    if (lane == 31) swarp[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        long long s = (lane < kT / 32) ? swarp[lane] : 0;
+        long long incs = s;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            long long y = __shfl_up_sync(0xffffffffu, incs, off);
+            if (lane >= off) incs += y;
+        }
+        if (lane < kT / 32) swarp[lane] = incs - s;
+        if (lane == kT / 32 - 1) swarp[kT / 32] = incs;
+    }
+    __syncthreads();
+    long long run = swarp[w] + inc - tsum;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        if (o + k < n) out[o + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = swarp[kT / 32];
+}
+
+// single CTA: exclusive scan of the block sums (in place)
+__global__ void __launch_bounds__(kT) k_scan_sums(int64_t* sums, int64_t nb) {
+    __shared__ long long swarp[kT / 32 + 1];
+    __shared__ long long s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t r = 0; r < nb; r += kT) {
+        const int64_t k = r + threadIdx.x;
+        const long long x = (k < nb) ? sums[k] : 0;
+        long long inc = x;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            long long y = __shfl_up_sync(0xffffffffu, inc, off);
+            if (lane >= off) inc += y;
+        }
+        if (lane == 31) swarp[w] = inc;
+        __syncthreads();
+        if (w == 0) {
+            long long s = (lane < kT / 32) ? swarp[lane] : 0;
+            long long incs = s;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                long long y = __shfl_up_sync(0xffffffffu, incs, off);
+                if (lane >= off) incs += y;
+            }
+            if (lane < kT / 32) swarp[lane] = incs - s;
+            if (lane == kT / 32 - 1) swarp[kT / 32] = incs;
+        }
+        __syncthreads();
+        if (k < nb) sums[k] = s_carry + swarp[w] + inc - x;
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += swarp[kT / 32];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[nb] = s_carry;
+}
+
+__global__ void __launch_bounds__(kT) k_scan_add(int64_t* out, int64_t n, const int64_t* sums) {
+    const int64_t o = (int64_t)blockIdx.x * kScanBlock + threadIdx.x * kScanPer;
+    const int64_t add = sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k)
+        if (o + k < n) out[o + k] += add;
+}
+
+int64_t scan_scratch_elems(int64_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }
+
+// out[0..n) = exclusive scan of in[0..n); out[n] = total.
+cudaError_t launch_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* scratch,
+                        cudaStream_t s, int64_t* launches) {
+    const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+    if (nb == 0) return cudaMemsetAsync(out, 0, sizeof(int64_t), s);
+    k_scan_local<<<(unsigned)nb, kT, 0, s>>>(in, out, n, scratch);
+    k_scan_sums<<<1, kT, 0, s>>>(scratch, nb);
+    k_scan_add<<<(unsigned)nb, kT, 0, s>>>(out, n, scratch);
+    // total
+    cudaError_t e = cudaMemcpyAsync(out + n, scratch + nb, sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+    *launches += 3;
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+/* ------------------------------------------------------------------ */
+/* the solver: one CTA runs one instance's whole schedule               */
+/* ------------------------------------------------------------------ */
+struct Inst {
+    int V;
+    int64_t base;          // first node index
+    const int64_t* row;    // row[v], v in [0, V]
+    const Slot* slot;
+    uint16_t* perm;
+    Slot* ef;              // EF arena of this instance (starts at row[0])
+};
+
+// Reduced cost of a slot of node v: D + 0.5*F[v1] + 0.5*F[v2] with v1<v2
+// (cuda_recompute_Edges, graph_cuda_grad.hpp:257-268).
+__device__ __forceinline__ double red_d(const Slot& s, int v, const double* F, double fv) {
+    const double fn = F[s.nbr];
+    return (v < s.nbr) ? (s.D + 0.5 * fv) + 0.5 * fn : (s.D + 0.5 * fn) + 0.5 * fv;
+}
+
+// cuda_get_Nodes_grad_R (graph_cuda_grad.hpp:321-340) over a node's EF list.
+__device__ __forceinline__ double ef_grad(const Inst& I, const int* efo, const double* F, int v) {
+    const int o0 = efo[v], n = efo[v + 1] - o0;
+    const double fv = F[v];
+    const Slot* e = I.ef + o0;
+    double v0 = red_d(e[0], v, F, fv), v1 = 1e6, v2 = 1e6;
+    for (int k = 1; k < n; ++k) {
+        const double x = red_d(e[k], v, F, fv);
+        if (x < v0) { v2 = v1; v1 = v0; v0 = x; continue; }
+        if (x < v1) { v2 = v1; v1 = x; continue; }
+        if (x < v2) { v2 = x; }
+    }
+    return -(v1 + v2) / 2;
+}
+
+__device__ __forceinline__ double pdv(const Inst& I, int64_t r0, const uint16_t* list, int k, int v,
+                                      const double* F, double fv) {
+    return red_d(I.slot[r0 + list[k]], v, F, fv);
+}
+
+// qpart_ptr_B (graph_cuda_partition.hpp:3-25), the bound tested first.  On
+// finite values it performs at most size/2 swaps; the pass cap only matters
+// for NaN values (where the reference loops forever) and keeps the kernel
+// finite.
+__device__ int qpart_b(const Inst& I, int64_t r0, int v, const double* F, int size, double avg) {
+    uint16_t* list = I.perm + r0;
+    const double fv = F[v];
+    int low = 0, high = size - 1, i = low, j = high;
+    for (int pass = 0; i < j && pass <= size; ++pass) {
+        while (i <= high && pdv(I, r0, list, i, v, F, fv) <= avg) i++;
+        while (j >= low && pdv(I, r0, list, j, v, F, fv) > avg) j--;
+        if (i < j) { const uint16_t t = list[i]; list[i] = list[j]; list[j] = t; }
+    }
+    return j + 1;
+}
+// qpart_ptr_EF (graph_cuda_partition.hpp:27-54): raise the threshold by 1
+// until at least ef_min entries qualify (bounded: see qpart_b).
+__device__ int qpart_ef(const Inst& I, int64_t r0, int v, const double* F, int size, double avg,
+                        int ef_min) {
+    if (size < ef_min) return size;  // the reference would not terminate
+    for (int bump = 0; bump < (1 << 20); ++bump) {
+        const int p = qpart_b(I, r0, v, F, size, avg);
+        if (p >= ef_min) return p;
+        avg += 1;
+    }
+    return size;
+}
+
+template <int T>
+struct Cta {
+    double* sred;
+    int* swarp;
+    int* s_carry;
+    long long* sredl;
+
+    // efo[0..V) holds counts -> exclusive offsets, efo[V] = total
+    __device__ void scan_counts(int* efo, int V) const {
+        if (threadIdx.x == 0) *s_carry = 0;
+        __syncthreads();
+        for (int r = 0; r < V; r += T) {
+            const int v = r + threadIdx.x;
+            const int c = (v < V) ? efo[v] : 0;
+            int tot;
+            const int ex = block_excl_scan<T>(c, swarp, &tot);
+            if (v < V) efo[v] = *s_carry + ex;
+            __syncthreads();
+            if (threadIdx.x == 0) *s_carry += tot;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) efo[V] = *s_carry;
+        __syncthreads();
+    }
+    // update_EF (graph_cuda.cu:229-252): copy each node's list prefix
+    __device__ void rebuild_ef(const Inst& I, const int* efo) const {
+        for (int v = threadIdx.x; v < I.V; v += T) {
+            const int64_t r0 = I.row[v];
+            const int o0 = efo[v], n = efo[v + 1] - o0;
+            for (int k = 0; k < n; ++k) I.ef[o0 + k] = I.slot[r0 + I.perm[r0 + k]];
+        }
+        __syncthreads();
+    }
+    __device__ double grad_max(const Inst& I, const int* efo, const double* F) const {
+        double m = 0.0;
+        for (int v = threadIdx.x; v < I.V; v += T) m = fmax(m, fabs(ef_grad(I, efo, F, v)));
+        return block_max<T>(m, sred);
+    }
+    // one Jacobi step: Fn = Fc + grad(Fc)
+    __device__ void jacobi(const Inst& I, const int* efo, const double* Fc, double* Fn) const {
+        for (int v = threadIdx.x; v < I.V; v += T) Fn[v] = Fc[v] + ef_grad(I, efo, Fc, v);
+        __syncthreads();
+    }
+};
+
+// Per-instance solver state in shared memory: two F buffers (Jacobi double
+// buffering) and the EF offsets efo[0..V].
+template <int T>
+struct Solver {
+    const Batch& B;
+    const DevParams& P;
+    const Inst& I;
+    const Cta<T>& C;
+    double* Fc;
+    double* Fn;
+    int* efo;
+    long long iters = 0;
+    long long wslots = 0;  // active slots read, summed over iterations (thread 0)
+    int checks = 0;
+    bool capped = false;
+
+    __device__ Solver(const Batch& b, const DevParams& p, const Inst& i, const Cta<T>& c, double* fa,
+                      double* fb, int* e)
+        : B(b), P(p), I(i), C(c), Fc(fa), Fn(fb), efo(e) {}
+
+    __device__ int deg(int v) const { return (int)(I.row[v + 1] - I.row[v]); }
+    __device__ void swap_f() { double* t = Fc; Fc = Fn; Fn = t; }
+    __device__ void jacobi() {
+        if (threadIdx.x == 0) wslots += efo[I.V];
+        C.jacobi(I, efo, Fc, Fn);
+        swap_f();
+        iters++;
+    }
+    // block_EF_iter_BLOCK (graph_cuda.cu:278-289): frozen nodes keep F
+    __device__ void jacobi_masked() {
+        for (int v = threadIdx.x; v < I.V; v += T) {
+            const double g = ef_grad(I, efo, Fc, v);
+            Fn[v] = (B.shift[I.base + v] != 0.0) ? Fc[v] : Fc[v] + g;
+        }
+        if (threadIdx.x == 0) wslots += efo[I.V];
+        __syncthreads();
+        swap_f();
+        iters++;
+    }
+    __device__ void finish_partition() {
+        __syncthreads();
+        C.scan_counts(efo, I.V);
+        C.rebuild_ef(I, efo);
+    }
+    // check_OPT + update_EF (graph_cuda.cu:229-271) with cuda_partition_v2
+    __device__ double check_opt() {
+        for (int v = threadIdx.x; v < I.V; v += T) {
+            const int d = deg(v);
+            efo[v] = (d < P.ef_small_deg) ? d : qpart_ef(I, I.row[v], v, Fc, d, P.ef_thr, P.ef_min);
+        }
+        finish_partition();
+        checks++;
+        return C.grad_max(I, efo, Fc);
+    }
+    // block_EF (graph_cuda.cu:308-338)
+    __device__ void block_ef(int N) {
+        const double MA = C.grad_max(I, efo, Fc);
+        int count_M = 0;
+        for (int it = 0; it < N; ++it) {
+            jacobi();
+            if (++count_M >= P.check_every) {
+                if (MA < P.error_B) break;
+                count_M = 0;
+            }
+        }
+    }
+    // block_GLOB (graph_cuda.cu:363-430)
+    __device__ void block_glob() {
+        for (int v = threadIdx.x; v < I.V; v += T) efo[v] = min(deg(v), P.glob_K);  // setvalue2V
+        finish_partition();
+        for (int go = 0; go < P.glob_rounds; ++go) {
+            for (int it = 0; it < P.glob_inner; ++it) jacobi();
+            // cuda_partition_v4 (graph_cuda_partition.hpp:89-115)
+            for (int v = threadIdx.x; v < I.V; v += T) {
+                const int d = deg(v);
+                if (d < P.glob_K) { efo[v] = d; continue; }
+                const int64_t r0 = I.row[v];
+                const double fv = Fc[v];
+                double avg = pdv(I, r0, I.perm + r0, 0, v, Fc, fv);
+                for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, I.perm + r0, k, v, Fc, fv));
+                efo[v] = qpart_ef(I, r0, v, Fc, d, avg, P.ef_min);
+            }
+            finish_partition();
+            if (C.grad_max(I, efo, Fc) < P.glob_tol) break;
+        }
+    }
+    // run_start_cuda (graph_cuda.cu:163-199)
+    __device__ double run_start() {
+        block_glob();
+        double M = check_opt();
+        int factor = P.factor0;
+        for (int go = 1; go <= P.max_rounds; ++go) {
+            block_ef(factor);
+            M = check_opt();
+            if (factor < P.factor_cap) factor += P.factor_step;
+            if (M < P.error_B) break;
+            if (iters > P.max_iters) { capped = true; break; }
+        }
+        return M;
+    }
+    // run_fix_cuda (graph_cuda.cu:204-226)
+    __device__ double run_fix() {
+        double M = check_opt();
+        for (int go = 1; go <= P.fix_rounds; ++go) {
+            block_ef(P.fix_factor);
+            M = check_opt();
+            if (M < P.error_B) break;
+            if (iters > P.max_iters) { capped = true; break; }
+        }
+        return M;
+    }
+    // Comb extraction (graph_cuda_comb.hpp:415-475), the device comb check and
+    // the primal; writes the per-node state for the host and the results.
+    __device__ void combs_and_primal(int b, double M, bool accumulate) {
+        const int V = I.V;
+        const double porog = P.porog;
+        int* ccnt = reinterpret_cast<int*>(Fn);  // Fn is free: room for 2V ints
+        int* lab = ccnt + V;
+        for (int v = threadIdx.x; v < V; v += T)  // cuda_partition_v3
+            ccnt[v] = qpart_b(I, I.row[v], v, Fc, efo[v + 1] - efo[v], P.comb_thr);
+        __syncthreads();
+        for (int v = threadIdx.x; v < V; v += T) {
+            const int64_t r0 = I.row[v];
+            const double fv = Fc[v];
+            bool has = false;
+            for (int k = 0; k < ccnt[v] && !has; ++k) {
+                const double d = pdv(I, r0, I.perm + r0, k, v, Fc, fv);
+                has = (d >= -porog && d <= porog);
+            }
+            lab[v] = has ? v : INT_MAX;
+        }
+        __syncthreads();
+        // a comb is a connected component of half edges rooted at its
+        // smallest node id (get_cuda_comb_size, graph_cuda_comb.hpp:320-392);
+        // min-label propagation over the half-edge frontier finds them
+        volatile int* vlab = lab;
+        int changed;
+        do {
+            changed = 0;
+            for (int v = threadIdx.x; v < V; v += T) {
+                int m = vlab[v];
+                if (m == INT_MAX) continue;
+                const int64_t r0 = I.row[v];
+                const double fv = Fc[v];
+                for (int k = 0; k < ccnt[v]; ++k) {
+                    const Slot s = I.slot[r0 + I.perm[r0 + k]];
+                    const double d = red_d(s, v, Fc, fv);
+                    if (d >= -porog && d <= porog) m = min(m, vlab[s.nbr]);
+                }
+                if (m < vlab[v]) { vlab[v] = m; changed = 1; }
+            }
+        } while (__syncthreads_or(changed));
+        // state for the host comb check
+        for (int v = threadIdx.x; v < V; v += T) {
+            B.F[I.base + v] = Fc[v];
+            B.efcnt[I.base + v] = efo[v + 1] - efo[v];
+            B.ccnt[I.base + v] = ccnt[v];
+        }
+        __syncthreads();
+        // comb check (comb::solve_simple, comb_thread.cpp:180-195) with the
+        // host's A/B rule (node::get_statusAB, node.cpp:49-57)
+        int* irr = efo;  // efo is no longer needed
+        for (int v = threadIdx.x; v < V; v += T) irr[v] = 0;
+        __syncthreads();
+        for (int v = threadIdx.x; v < V; v += T) {
+            if (lab[v] == INT_MAX) continue;
+            const int64_t r0 = I.row[v], r1 = I.row[v + 1];
+            const double fv = Fc[v];
+            int A = 0, Bc = 0;
+            for (int64_t a = r0; a < r1; ++a) {
+                const double d = red_d(I.slot[a], v, Fc, fv);
+                if (d < porog) { if (d > -porog) Bc++; else A++; }
+            }
+            if (4 - 2 * A - Bc != 0) irr[lab[v]] = 1;
+        }
+        __syncthreads();
+        long long nc = 0, ni = 0;
+        for (int v = threadIdx.x; v < V; v += T)
+            if (lab[v] == v) { nc++; ni += irr[v]; }
+        nc = block_sum_ll<T>(nc, C.sredl);
+        ni = block_sum_ll<T>(ni, C.sredl);
+        // primal (graph_cuda.cu:135-147): x = 1 on A edges, 1/2 on the B edges
+        // of regular combs; OVAL = sum x*Do, MAX edge rank (graph_tour.hpp:165-184)
+        double lp = 0.0, dual_neg = 0.0, fsum = 0.0;
+        long long maxr = -1, viol = 0;
+        for (int v = threadIdx.x; v < V; v += T) {
+            const int64_t r0 = I.row[v], r1 = I.row[v + 1];
+            const double fv = Fc[v];
+            fsum += fv;
+            float degsum = 0.0f;
+            bool any = false;
+            for (int64_t a = r0; a < r1; ++a) {
+                const Slot s = I.slot[a];
+                const double d = red_d(s, v, Fc, fv);
+                const double x = (d < porog) ? ((d > -porog) ? 0.5 : 1.0) : 0.0;
+                B.xcode[a] = (uint8_t)(x == 1.0 ? 2 : (x == 0.5 ? 1 : 0));
+                degsum += (float)x;
+                any |= (x != 0.0);
+                if (s.nbr > v) {
+                    lp += x * B.s_cost[a];
+                    dual_neg += fmin(0.0, d);
+                    if (x != 0.0) maxr = max(maxr, (long long)min((int)(a - r0), B.mirror[a]));
+                }
+            }
+            if (any && !(degsum > 2.0f - 1e-2f && degsum < 2.0f + 1e-2f)) viol++;
+        }
+        lp = block_sum<T>(lp, C.sred);
+        dual_neg = block_sum<T>(dual_neg, C.sred);
+        fsum = block_sum<T>(fsum, C.sred);
+        maxr = block_max_ll<T>(maxr, C.sredl);
+        viol = block_sum_ll<T>(viol, C.sredl);
+        if (threadIdx.x == 0) {
+            const double dmin = __longlong_as_double((long long)B.dmin_bits[b]);
+            B.n_edges[b] = (int32_t)((I.row[V] - I.row[0]) / 2);
+            B.n_combs[b] = (int32_t)nc;
+            B.n_irr[b] = (int32_t)ni;
+            B.max_rank[b] = (int32_t)maxr;
+            B.deg_viol[b] = (int32_t)viol;
+            B.iters[b] = (accumulate ? B.iters[b] : 0) + iters;
+            B.work_nodes[b] = (accumulate ? B.work_nodes[b] : 0) + iters * (long long)V;
+            B.work_slots[b] = (accumulate ? B.work_slots[b] : 0) + wslots;
+            B.checks[b] = (accumulate ? B.checks[b] : 0) + checks;
+            B.max_grad[b] = M;
+            B.dual[b] = dmin * (-fsum + dual_neg);
+            if (capped) { B.status[b] = F2M_ERR_NOT_CONVERGED; B.lp[b] = NAN; }
+            else if (ni > 0) { B.status[b] = kNeedsHost; B.lp[b] = NAN; }
+            else { B.status[b] = F2M_OK; B.lp[b] = lp; }
+        }
+        __syncthreads();
+    }
+};
+
+__device__ __forceinline__ Inst make_inst(const Batch& B, int b) {
+    Inst I;
+    I.V = B.Vn[b];
+    I.base = B.offs[b];
+    I.row = B.row + I.base;
+    I.slot = B.slot;
+    I.perm = B.perm;
+    I.ef = B.ef + I.row[0];
+    return I;
+}
+
+// Persistent CTAs take instances from a work counter, largest first.
+template <int T, bool REFIT>
+__global__ void __launch_bounds__(T) k_solve(Batch B, DevParams P, int vcap) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* FA = reinterpret_cast<double*>(smem_raw);
+    double* FB = FA + vcap;
+    int* efo = reinterpret_cast<int*>(FB + vcap);
+    __shared__ double sred[T / 32];
+    __shared__ long long sredl[T / 32];
+    __shared__ int swarp[T / 32 + 1];
+    __shared__ int s_carry;
+    __shared__ int s_item;
+    Cta<T> C{sred, swarp, &s_carry, sredl};
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(B.queue, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= B.n_items) return;
+        const int b = B.order[item];
+        const int st = B.status[b];
+        if (REFIT ? (st != F2M_OK && st != kNeedsHost) : (st != F2M_OK)) continue;
+        const Inst I = make_inst(B, b);
+        if (I.V > vcap) {
+            if (threadIdx.x == 0) B.status[b] = F2M_ERR_CAPACITY;
+            __syncthreads();
+            continue;
+        }
+        Solver<T> S(B, P, I, C, FA, FB, efo);
+        double M;
+        if (!REFIT) {
+            for (int v = threadIdx.x; v < I.V; v += T) FA[v] = 0.0;  // graph_cuda_init.hpp:183
+            __syncthreads();
+            M = S.run_start();
+        } else {
+            // cuda_IRREGULAR_B_recompute (graph_cuda_comb.hpp:542-574): shift the
+            // potentials of irregular combs, 20 frozen iterations, run_fix
+            for (int v = threadIdx.x; v < I.V; v += T) {
+                FA[v] = B.F[I.base + v] + B.shift[I.base + v];
+                efo[v] = B.efcnt[I.base + v];
+            }
+            __syncthreads();
+            C.scan_counts(efo, I.V);  // the EF arena still holds the last update_EF
+            for (int go = 0; go < P.frozen_iters; ++go) S.jacobi_masked();
+            M = S.run_fix();
+        }
+        S.combs_and_primal(b, M, REFIT);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* host launchers                                                       */
+/* ------------------------------------------------------------------ */
+cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches) {
+    k_prep<<<B.n_inst, kT, 0, s>>>(B);
+    ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_knn(const Batch& B, cudaStream_t s, int64_t* launches) {
+    k_cutoff<<<B.n_chunks, kT, 0, s>>>(B);
+    ++*launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (B.N <= 16) k_select<16><<<B.n_chunks, kT, 0, s>>>(B);
+    else if (B.N <= 32) k_select<32><<<B.n_chunks, kT, 0, s>>>(B);
+    else if (B.N <= 64) k_select<64><<<B.n_chunks, kT, 0, s>>>(B);
+    else if (B.N <= 128) k_select<128><<<B.n_chunks, kT, 0, s>>>(B);
+    else k_select<256><<<B.n_chunks, kT, 0, s>>>(B);
+    ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_graph(const Batch& B, int64_t* deg, int64_t* scan_scratch, cudaStream_t s,
+                         int64_t* launches) {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(B.rev, 0, sizeof(int32_t) * B.n_total, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(B.cursor, 0, sizeof(int32_t) * B.n_total, s)) != cudaSuccess) return e;
+    k_graph_rev<<<B.n_chunks, kT, 0, s>>>(B);
+    k_graph_deg<<<B.n_chunks, kT, 0, s>>>(B, deg);
+    *launches += 2;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_scan(deg, B.row, B.n_total, scan_scratch, s, launches)) != cudaSuccess) return e;
+    k_graph_fill<<<B.n_chunks, kT, 0, s>>>(B);
+    k_graph_sort<<<B.n_chunks, kT, 0, s>>>(B);
+    k_graph_mirror<<<B.n_chunks, kT, 0, s>>>(B);
+    *launches += 3;
+    return cudaGetLastError();
+}
+
+size_t solve_smem_bytes(int32_t v_max) {
+    return (size_t)v_max * 2 * sizeof(double) + ((size_t)v_max + 1) * sizeof(int);
+}
+int32_t solve_max_nodes() { return 9000; }
+
+template <int T, bool R>
+static int occupancy(size_t smem) {
+    int nb = 0;
+    cudaFuncSetAttribute(k_solve<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_solve<T, R>, T, smem);
+    return nb;
+}
+int solve_blocks_per_sm(int threads, size_t smem) {
+    if (threads == 512) return occupancy<512, false>(smem);
+    if (threads == 128) return occupancy<128, false>(smem);
+    return occupancy<256, false>(smem);
+}
+
+template <bool R>
+static cudaError_t launch_solver(const Batch& B, const DevParams& P, int32_t v_max, int threads,
+                                 cudaStream_t s, int64_t* launches) {
+    if (B.n_items <= 0) return cudaSuccess;
+    const size_t smem = solve_smem_bytes(v_max);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 0;
+    if (threads == 512) per_sm = occupancy<512, R>(smem);
+    else if (threads == 128) per_sm = occupancy<128, R>(smem);
+    else per_sm = occupancy<256, R>(smem);
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    int grid = sms * per_sm;
+    if (grid > B.n_items) grid = B.n_items;
+    cudaError_t e = cudaMemsetAsync(B.queue, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess) return e;
+    if (threads == 512) k_solve<512, R><<<grid, 512, smem, s>>>(B, P, v_max);
+    else if (threads == 128) k_solve<128, R><<<grid, 128, smem, s>>>(B, P, v_max);
+    else k_solve<256, R><<<grid, 256, smem, s>>>(B, P, v_max);
+    ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_solve(const Batch& B, const DevParams& P, int32_t v_max, int threads,
+                         cudaStream_t s, int64_t* launches) {
+    return launch_solver<false>(B, P, v_max, threads, s, launches);
+}
+cudaError_t launch_refit(const Batch& B, const DevParams& P, int32_t v_max, int threads,
+                         cudaStream_t s, int64_t* launches) {
+    return launch_solver<true>(B, P, v_max, threads, s, launches);
+}
+
+}  // namespace f2m

@@ -1,0 +1,1324 @@
+// f2m_b200 host runtime: the C ABI of include/f2m.h.
+//
+// Device work (kNN, graph build, descent, partitions, combs, primal) runs in
+// the kernels of f2m_kernels.cu.  The host side mirrors the reference's own
+// host stages: TSPLIB parsing (FXY.hpp:186-309), the graph assembly in the
+// reference's node order (graph_tour.hpp:28-110), the host comb check with
+// its Ax=b solver (graph_cuda_comb.hpp:121-147, E_thread.cpp, V_thread.cpp,
+// comb_thread.cpp, Ax_b.cpp), the repair-loop driver (graph_cuda.cu:69-126)
+// and the output files (graph_tour.hpp:186-241, FXY.hpp:146-183).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "f2m_internal.h"
+
+using namespace f2m;
+
+/* ------------------------------------------------------------------ */
+/* context                                                              */
+/* ------------------------------------------------------------------ */
+namespace {
+
+struct Arena {
+    char* base = nullptr;
+    size_t cap = 0, used = 0;
+    template <class T>
+    T* take(size_t n) {
+        size_t off = (used + 255) & ~(size_t)255;
+        used = off + n * sizeof(T);
+        return base ? reinterpret_cast<T*>(base + off) : nullptr;
+    }
+};
+
+}  // namespace
+
+struct f2m_ctx {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    char* dev = nullptr;
+    size_t dev_cap = 0;
+    char* pinned = nullptr;
+    size_t pinned_cap = 0;
+    // CUDA events around the phases of the last batched call
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool timed = false;
+    Batch last{};  // pointers of the last batched call (for the work counters)
+};
+
+namespace {
+
+f2m_status fail(f2m_ctx* c, f2m_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+f2m_status cuda_fail(f2m_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, F2M_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define F2M_CUDA(call)                                                  \
+    do {                                                                \
+        cudaError_t e_ = (call);                                        \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);        \
+    } while (0)
+
+cudaError_t ensure_device(f2m_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->dev_cap) return cudaSuccess;
+    if (ctx->dev) cudaFree(ctx->dev);
+    ctx->dev = nullptr;
+    ctx->dev_cap = 0;
+    size_t want = bytes + bytes / 8;
+    cudaError_t e = cudaMalloc(&ctx->dev, want);
+    if (e != cudaSuccess) return e;
+    ctx->dev_cap = want;
+    return cudaSuccess;
+}
+cudaError_t ensure_pinned(f2m_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->pinned_cap) return cudaSuccess;
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_cap = 0;
+    size_t want = bytes + bytes / 8 + 4096;
+    cudaError_t e = cudaHostAlloc(&ctx->pinned, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) return e;
+    ctx->pinned_cap = want;
+    return cudaSuccess;
+}
+
+DevParams to_dev(const f2m_params& p) {
+    DevParams d;
+    d.error_B = p.error_B;
+    d.porog = p.error_B * p.error_B_comb;  // graph_cuda_comb.hpp:156
+    d.glob_tol = p.glob_tol;
+    d.ef_thr = p.ef_thr;
+    d.comb_thr = p.comb_thr;
+    d.glob_K = p.glob_K;
+    d.glob_rounds = p.glob_rounds;
+    d.glob_inner = p.glob_inner;
+    d.factor0 = p.factor0;
+    d.factor_step = p.factor_step;
+    d.factor_cap = p.factor_cap;
+    d.max_rounds = p.max_rounds;
+    d.fix_rounds = p.fix_rounds;
+    d.fix_factor = p.fix_factor;
+    d.check_every = p.check_every;
+    d.frozen_iters = p.frozen_iters;
+    d.ef_small_deg = p.ef_small_deg;
+    d.ef_min = p.ef_min;
+    d.max_iters = p.max_iters;
+    return d;
+}
+
+/* ------------------------------------------------------------------ */
+/* batch plan + device layout                                           */
+/* ------------------------------------------------------------------ */
+constexpr int kChunk = 256;
+
+struct Plan {
+    int32_t n_inst = 0;
+    int64_t n_total = 0;
+    int32_t max_n = 0;
+    int32_t N = 0;
+    std::vector<int32_t> chunk_inst, chunk_start, order;
+    int64_t S_cap = 0;
+};
+
+void make_plan(Plan& pl, int32_t n_inst, const int64_t* offs, int32_t N) {
+    pl.n_inst = n_inst;
+    pl.N = N;
+    pl.n_total = offs[n_inst] - offs[0];
+    pl.max_n = 0;
+    pl.chunk_inst.clear();
+    pl.chunk_start.clear();
+    for (int32_t b = 0; b < n_inst; ++b) {
+        const int32_t n = (int32_t)(offs[b + 1] - offs[b]);
+        pl.max_n = std::max(pl.max_n, n);
+        for (int32_t s = 0; s < n; s += kChunk) {
+            pl.chunk_inst.push_back(b);
+            pl.chunk_start.push_back(s);
+        }
+    }
+    pl.order.resize(n_inst);
+    std::iota(pl.order.begin(), pl.order.end(), 0);
+    std::stable_sort(pl.order.begin(), pl.order.end(), [&](int a, int b) {
+        return offs[a + 1] - offs[a] > offs[b + 1] - offs[b];
+    });
+    const int64_t Neff = std::min<int64_t>(N, std::max<int32_t>(pl.max_n - 1, 1));
+    pl.S_cap = 2 * Neff * std::max<int64_t>(pl.n_total, 1);
+}
+
+// Carves every buffer of a batched call out of one arena.  With A.base ==
+// nullptr it only measures.
+void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, int64_t** scan_scratch,
+           int32_t** d_chunk_inst, int32_t** d_chunk_start, int32_t** d_order) {
+    const int64_t n = std::max<int64_t>(pl.n_total, 1);
+    const int32_t ni = pl.n_inst;
+    const int64_t S = std::max<int64_t>(pl.S_cap, 1);
+    const int64_t nN = n * pl.N;
+    B.n_inst = ni;
+    B.N = pl.N;
+    B.N_cut = pl.N;
+    B.n_total = (int32_t)pl.n_total;
+    if (own_inputs) {
+        B.offs = A.take<int64_t>(ni + 1);
+        B.X_in = A.take<double>(n);
+        B.Y_in = A.take<double>(n);
+    }
+    B.K_in = nullptr;
+    B.Pr = A.take<double2>(n);
+    B.P = A.take<double2>(n);
+    B.K = A.take<int32_t>(n);
+    B.dup_of = A.take<int32_t>(n);
+    B.Vn = A.take<int32_t>(ni);
+    B.spn = A.take<double>(ni);
+    B.dmin_bits = A.take<unsigned long long>(ni);
+    B.status = A.take<int32_t>(ni);
+    B.cut = A.take<double>(n);
+    B.stat = A.take<int32_t>(n);
+    B.ntop = A.take<int32_t>(n);
+    B.top_nbr = A.take<int32_t>(nN);
+    B.top_cost = A.take<double>(nN);
+    B.top_em = A.take<int32_t>(nN);
+    B.top_oth = A.take<int32_t>(nN);
+    B.rev = A.take<int32_t>(n);
+    B.cursor = A.take<int32_t>(n);
+    B.row = A.take<int64_t>(n + 1);
+    B.s_nbr = A.take<int32_t>(S);
+    B.s_cost = A.take<double>(S);
+    B.s_em = A.take<int32_t>(S);
+    B.s_oth = A.take<int32_t>(S);
+    B.slot = A.take<Slot>(S);
+    B.perm = A.take<uint16_t>(S);
+    B.mirror = A.take<int32_t>(S);
+    B.ef = A.take<Slot>(S);
+    B.xcode = A.take<uint8_t>(S);
+    B.S_cap = S;
+    B.F = A.take<double>(n);
+    B.efcnt = A.take<int32_t>(n);
+    B.ccnt = A.take<int32_t>(n);
+    B.shift = A.take<double>(n);
+    B.lp = A.take<double>(ni);
+    B.n_edges = A.take<int32_t>(ni);
+    B.n_combs = A.take<int32_t>(ni);
+    B.n_irr = A.take<int32_t>(ni);
+    B.max_rank = A.take<int32_t>(ni);
+    B.deg_viol = A.take<int32_t>(ni);
+    B.iters = A.take<int64_t>(ni);
+    B.work_nodes = A.take<int64_t>(ni);
+    B.work_slots = A.take<int64_t>(ni);
+    B.checks = A.take<int32_t>(ni);
+    B.max_grad = A.take<double>(ni);
+    B.dual = A.take<double>(ni);
+    *d_chunk_inst = A.take<int32_t>(pl.chunk_inst.size() + 1);
+    *d_chunk_start = A.take<int32_t>(pl.chunk_start.size() + 1);
+    *d_order = A.take<int32_t>(ni + 1);
+    B.chunk_inst = *d_chunk_inst;
+    B.chunk_start = *d_chunk_start;
+    B.n_chunks = (int32_t)pl.chunk_inst.size();
+    B.order = *d_order;
+    B.n_items = ni;
+    B.queue = A.take<int32_t>(2);
+    *deg = A.take<int64_t>(n + 1);
+    *scan_scratch = A.take<int64_t>(scan_scratch_elems(n) + 1);
+}
+
+int pick_threads(const f2m_params& p, int32_t max_n) {
+    if (p.threads == 128 || p.threads == 256 || p.threads == 512) return p.threads;
+    return max_n > 2048 ? 512 : 256;
+}
+
+/* ------------------------------------------------------------------ */
+/* host comb check and repair loop (the reference's host stage)          */
+/* ------------------------------------------------------------------ */
+// One instance pulled back to the host, in the reference's data model.
+struct HostInst {
+    int V = 0, E = 0;
+    std::vector<int> label;            // internal id -> TSPLIB label
+    std::vector<int64_t> row;          // V+1 local slot offsets
+    std::vector<int> nbr;              // per slot
+    std::vector<double> Dn, cost;      // per slot
+    std::vector<uint16_t> perm;        // per slot (current list order)
+    std::vector<int> mirror;           // per slot
+    std::vector<int> slot_edge;        // per slot -> edge id
+    std::vector<int> ev1, ev2, el1, el2, rank1, rank2;  // per edge
+    std::vector<double> eD, eDo;       // per edge
+    std::vector<double> F;
+    std::vector<int> efcnt, ccnt;
+    double dmin = 0;
+};
+
+// Edge ids in the reference's global order: slots with nbr>v, sorted by the
+// candidate key (cost, emitter, partner) (FXY.hpp:100-101, graph_tour.hpp:28-90).
+void number_edges(HostInst& H, const std::vector<int>& em, const std::vector<int>& oth) {
+    struct K { double c; int e, o; int v; int64_t s; };
+    std::vector<K> ks;
+    for (int v = 0; v < H.V; ++v)
+        for (int64_t a = H.row[v]; a < H.row[v + 1]; ++a)
+            if (H.nbr[a] > v) ks.push_back({H.cost[a], em[a], oth[a], v, a});
+    std::sort(ks.begin(), ks.end(), [](const K& x, const K& y) {
+        if (x.c != y.c) return x.c < y.c;
+        if (x.e != y.e) return x.e < y.e;
+        return x.o < y.o;
+    });
+    H.E = (int)ks.size();
+    H.slot_edge.assign(H.nbr.size(), -1);
+    H.ev1.resize(H.E); H.ev2.resize(H.E); H.el1.resize(H.E); H.el2.resize(H.E);
+    H.rank1.resize(H.E); H.rank2.resize(H.E); H.eD.resize(H.E); H.eDo.resize(H.E);
+    for (int e = 0; e < H.E; ++e) {
+        const int v = ks[e].v;
+        const int64_t a = ks[e].s;
+        const int u = H.nbr[a];
+        H.slot_edge[a] = e;
+        H.slot_edge[H.row[u] + H.mirror[a]] = e;
+        H.ev1[e] = v; H.ev2[e] = u;
+        H.eD[e] = H.Dn[a]; H.eDo[e] = H.cost[a];
+        const int rv = (int)(a - H.row[v]), ru = H.mirror[a];
+        if (H.label[v] < H.label[u]) { H.el1[e] = v; H.el2[e] = u; H.rank1[e] = rv; H.rank2[e] = ru; }
+        else { H.el1[e] = u; H.el2[e] = v; H.rank1[e] = ru; H.rank2[e] = rv; }
+    }
+}
+
+struct HostCheck {
+    HostInst& H;
+    double vb;
+    std::vector<std::vector<int>> node_edges, eA, eB;
+    std::vector<int> sA, sB;
+    std::vector<int> irrB;  // comb_IRREGULAR_B, kept across checks (F2M.h:166)
+    struct CombH {
+        std::unordered_map<int, int> nodes;
+        std::unordered_map<int, float> XB;
+        int STATUS = 1, AxB_status = 1;
+    };
+    std::vector<CombH> Combs;
+    std::vector<std::vector<int>> comb_V;  // BFS order
+    int irr_a = 0;
+
+    HostCheck(HostInst& h, double band) : H(h), vb(band) {
+        node_edges.resize(H.V);
+        for (int v = 0; v < H.V; ++v)
+            for (int64_t a = H.row[v]; a < H.row[v + 1]; ++a) node_edges[v].push_back(H.slot_edge[a]);
+    }
+    double dgpu(int64_t a, int v) const {  // cuda_recompute_Edges
+        const int u = H.nbr[a];
+        return (v < u) ? (H.Dn[a] + 0.5 * H.F[v]) + 0.5 * H.F[u] : (H.Dn[a] + 0.5 * H.F[u]) + 0.5 * H.F[v];
+    }
+    // get_cuda_comb_size/fill BFS order from each component's smallest id
+    // over the comb prefix (graph_cuda_comb.hpp:258-392)
+    void extract_combs() {
+        comb_V.clear();
+        std::vector<int> seen(H.V, 0);
+        std::vector<int> eseen(H.E, 0);
+        for (int r = 0; r < H.V; ++r) {
+            if (seen[r]) continue;
+            std::vector<int> fn{r}, A{r}, Bn;
+            bool any = false, lower = false;
+            std::vector<int> touched{r};
+            seen[r] = 1;
+            while (!A.empty() && !lower) {
+                Bn.clear();
+                for (int lA : A) {
+                    const int64_t r0 = H.row[lA];
+                    for (int k = 0; k < H.ccnt[lA]; ++k) {
+                        const int64_t a = r0 + H.perm[r0 + k];
+                        const double d = dgpu(a, lA);
+                        if (d >= -vb && d <= vb) {
+                            any = true;
+                            const int v = H.nbr[a];
+                            if (v < r) { lower = true; break; }
+                            if (!seen[v]) { seen[v] = 1; touched.push_back(v); Bn.push_back(v); fn.push_back(v); }
+                        }
+                    }
+                    if (lower) break;
+                }
+                std::swap(A, Bn);
+            }
+            if (lower) {
+                for (int t : touched) if (t != r) seen[t] = 0;  // revisit from its own root later
+                seen[r] = 1;
+                continue;
+            }
+            if (any) comb_V.push_back(fn);
+        }
+    }
+    // Ax_b (Ax_b.cpp:19-158)
+    struct AxB {
+        std::vector<std::vector<int>> Ai, Av;
+        std::vector<int> b;
+        std::vector<double> d, Aj, x, x_grad, b_grad;
+        double d_max_error = 0;
+        int go_max = 0, i_count = 0, j_count = 0;
+        explicit AxB(const std::vector<int>& A) {
+            int j = 0, norm = 0;
+            std::vector<int> Aij, Avj;
+            for (size_t k = 0; k + 1 < A.size(); k += 2) {
+                const int i = A[k], v = A[k + 1];
+                if (!(i >= -1)) break;
+                if (i > i_count) i_count = i;
+                if (i == -1) {
+                    b.push_back(v);
+                    Aj.push_back(std::sqrt((double)norm));
+                    norm = 0;
+                    j++;
+                    Ai.push_back(Aij); Av.push_back(Avj);
+                    Aij.clear(); Avj.clear();
+                } else {
+                    Aij.push_back(i); Avj.push_back(v);
+                    norm += v * v;
+                }
+            }
+            j_count = j;
+            x.assign(i_count + 1, 0.0);
+            x_grad.assign(i_count + 1, 0.0);
+            d.assign(j_count, 0.0);
+            b_grad.assign(j_count, 0.0);
+        }
+        double ax(int j, const std::vector<double>& X) const {
+            double v = 0;
+            for (size_t i = 0; i < Ai[j].size(); i++) v += Av[j][i] * X[Ai[j][i]];
+            return v;
+        }
+        void solve() {
+            go_max = 0;
+            for (int go = 1; go < 1000; go++) {
+                std::fill(x_grad.begin(), x_grad.end(), 0.0);
+                d_max_error = 0;
+                for (size_t j = 0; j < Ai.size(); j++) {
+                    d[j] = (ax((int)j, x) - b[j]) / Aj[j];
+                    if (std::fabs(d[j]) > d_max_error) d_max_error = std::fabs(d[j]);
+                    for (size_t i = 0; i < Ai[j].size(); i++) x_grad[Ai[j][i]] += Av[j][i] * d[j] / Aj[j];
+                }
+                if (d_max_error < 1e-8) { go_max = go; break; }
+                for (size_t j = 0; j < Ai.size(); j++) b_grad[j] = ax((int)j, x_grad);
+                double gg = 0, gd = 0;
+                for (size_t j = 0; j < b_grad.size(); j++) gg += b_grad[j] * b_grad[j];
+                for (size_t j = 0; j < d.size(); j++) gd += d[j] * b_grad[j];
+                const double alfa = -gd / gg;
+                for (size_t j = 0; j < x.size(); j++) x[j] += x_grad[j] * alfa;
+            }
+        }
+    };
+    // host_combs_check (graph_cuda_comb.hpp:121-147)
+    int check() {
+        const int E = H.E;
+        std::vector<double> dcpu(E);
+        for (int e = 0; e < E; ++e)  // E_thread.cpp:39
+            dcpu[e] = H.eD[e] + H.F[H.el1[e]] / 2 + H.F[H.el2[e]] / 2;
+        eA.assign(H.V, {});
+        eB.assign(H.V, {});
+        sA.assign(H.V, 0);
+        sB.assign(H.V, 0);
+        for (int v = 0; v < H.V; ++v) {  // node::resort + node::get_statusAB
+            auto& ed = node_edges[v];
+            std::sort(ed.begin(), ed.end(), [&](int a, int b) { return dcpu[a] < dcpu[b]; });
+            for (int e : ed) {
+                if (dcpu[e] < vb) {
+                    if (dcpu[e] > -vb) { sB[v]++; eB[v].push_back(e); }
+                    else { sA[v]++; eA[v].push_back(e); }
+                } else break;
+            }
+        }
+        extract_combs();
+        Combs.clear();
+        Combs.resize(comb_V.size());
+        std::vector<int> irrA;
+        for (size_t c = 0; c < comb_V.size(); ++c) {  // COMB_thread + solve_simple
+            auto& C = Combs[c];
+            for (int v : comb_V[c]) C.nodes[v]++;
+            for (auto& kv : C.nodes)
+                if (4 - 2 * sA[kv.first] - sB[kv.first] != 0) { C.STATUS = -1; break; }
+            if (C.STATUS == 1)
+                for (auto& kv : C.nodes)
+                    for (int e : eB[kv.first]) C.XB[e] = 0.5f;
+            else irrA.push_back((int)c);
+        }
+        irr_a = (int)irrA.size();
+        if (!irrA.empty()) {
+            for (int c : irrA) {  // comb::solve_AxB (comb_thread.cpp:272-304)
+                auto& C = Combs[c];
+                std::vector<int> rows;
+                std::unordered_map<int, int> mapX, mapXR;
+                int countX = 0;
+                for (auto& kv : C.nodes) {
+                    for (int e : eB[kv.first]) {
+                        int i;
+                        auto it = mapX.find(e);
+                        if (it != mapX.end()) i = it->second;
+                        else { i = countX; mapXR[i] = e; mapX[e] = i; countX++; }
+                        rows.push_back(i);
+                        rows.push_back(1);
+                    }
+                    rows.push_back(-1);
+                    rows.push_back(2 - (int)eA[kv.first].size());
+                }
+                AxB ab(rows);
+                ab.solve();
+                C.AxB_status = ab.go_max;
+                for (size_t j = 0; j < ab.x.size(); j++) C.XB[mapXR[(int)j]] = (float)ab.x[j];
+            }
+            irrB.clear();  // get_comb_IRREGULAR_B
+            for (size_t c = 0; c < Combs.size(); ++c)
+                if (Combs[c].AxB_status == 0) irrB.push_back((int)c);
+        }
+        return (int)irrB.size();
+    }
+    // shift_comb_IRREGULAR_B (graph_cuda_comb.hpp:484-522) with the device A/B
+    // rule (cuda_get_Nodes_StatAB, graph_cuda_grad.hpp:274-295)
+    void shifts(double shiftV, int type, std::vector<double>& sh) const {
+        sh.assign(H.V, 0.0);
+        for (int c : irrB) {
+            if (c < 0 || c >= (int)comb_V.size()) continue;  // stale index
+            for (int nid : comb_V[c]) {
+                const int64_t r0 = H.row[nid];
+                int A = 0, B = 0;
+                for (int k = 0; k < H.ccnt[nid]; ++k) {
+                    const double d = dgpu(r0 + H.perm[r0 + k], nid);
+                    if (d < -vb) A++;
+                    else if (d < vb) B++;
+                }
+                const int v = 4 - 2 * A - B;
+                if (v != 0) {
+                    sh[nid] += shiftV * (v > 0 ? 1 : -1);
+                    if (type == 1) break;
+                }
+            }
+        }
+    }
+};
+
+}  // namespace
+
+/* ------------------------------------------------------------------ */
+/* result object                                                        */
+/* ------------------------------------------------------------------ */
+struct f2m_result {
+    int32_t status = F2M_OK;
+    std::string err;
+    HostInst H;
+    std::vector<double> x;               // per edge
+    std::unordered_map<int, double> X;   // graph::X in insertion order
+    double lp = NAN;
+    int32_t max_rank = 0;
+    double seconds = 0;
+    f2m_stats st{};
+    // inputs kept for the output files
+    std::vector<int> dup_label_of;       // per input point: label of the kept copy or -1
+    std::vector<int> in_label;
+};
+
+namespace {
+
+/* ------------------------------------------------------------------ */
+/* one batched device pass                                              */
+/* ------------------------------------------------------------------ */
+struct DevCall {
+    Plan pl;
+    Batch B{};
+    int64_t* deg = nullptr;
+    int64_t* scan = nullptr;
+    int32_t *ci = nullptr, *cs = nullptr, *ord = nullptr;
+    int threads = 256;
+    int32_t vcap = 0;
+};
+
+f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h_offs, int32_t top_k,
+                      const f2m_params& prm, bool own_inputs) {
+    make_plan(C.pl, n_inst, h_offs, top_k);
+    if (C.pl.max_n > solve_max_nodes())
+        return fail(ctx, F2M_ERR_CAPACITY, "instance larger than the CTA solver limit (" +
+                                               std::to_string(solve_max_nodes()) + " points)");
+    Arena A;
+    carve(A, C.B, C.pl, own_inputs, &C.deg, &C.scan, &C.ci, &C.cs, &C.ord);
+    F2M_CUDA(ensure_device(ctx, A.used));
+    A.base = ctx->dev;
+    A.used = 0;
+    carve(A, C.B, C.pl, own_inputs, &C.deg, &C.scan, &C.ci, &C.cs, &C.ord);
+    C.threads = pick_threads(prm, C.pl.max_n);
+    C.vcap = std::max<int32_t>(C.pl.max_n, 4);
+    // work lists through pinned staging
+    const size_t nc = C.pl.chunk_inst.size();
+    const size_t bytes = (2 * nc + n_inst) * sizeof(int32_t);
+    F2M_CUDA(ensure_pinned(ctx, bytes));
+    int32_t* hp = reinterpret_cast<int32_t*>(ctx->pinned);
+    std::memcpy(hp, C.pl.chunk_inst.data(), nc * sizeof(int32_t));
+    std::memcpy(hp + nc, C.pl.chunk_start.data(), nc * sizeof(int32_t));
+    std::memcpy(hp + 2 * nc, C.pl.order.data(), n_inst * sizeof(int32_t));
+    F2M_CUDA(cudaMemcpyAsync(C.ci, hp, nc * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(C.cs, hp + nc, nc * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(C.ord, hp + 2 * nc, n_inst * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+    return F2M_OK;
+}
+
+f2m_status run_device(f2m_ctx* ctx, DevCall& C, const f2m_params& prm, bool build_graph, bool solve) {
+    F2M_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+    F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
+    F2M_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+    F2M_CUDA(launch_knn(C.B, ctx->stream, &ctx->launches));
+    F2M_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
+    if (build_graph) F2M_CUDA(launch_graph(C.B, C.deg, C.scan, ctx->stream, &ctx->launches));
+    F2M_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+    if (solve) F2M_CUDA(launch_solve(C.B, to_dev(prm), C.vcap, C.threads, ctx->stream, &ctx->launches));
+    F2M_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
+    ctx->timed = true;
+    ctx->last = C.B;
+    return F2M_OK;
+}
+
+template <class T>
+f2m_status d2h(f2m_ctx* ctx, std::vector<T>& v, const T* src, size_t n) {
+    v.resize(n);
+    if (n) F2M_CUDA(cudaMemcpyAsync(v.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    return F2M_OK;
+}
+template <class T>
+f2m_status h2d(f2m_ctx* ctx, T* dst, const std::vector<T>& v) {
+    if (!v.empty()) F2M_CUDA(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    return F2M_OK;
+}
+
+// Pull instance b (device-built graph, node ids = de-duplicated input order).
+f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, bool with_keys) {
+    const Batch& B = C.B;
+    int32_t V = 0;
+    int64_t base = 0;
+    F2M_CUDA(cudaMemcpyAsync(&V, B.Vn + b, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(&base, B.offs + b, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    unsigned long long db = 0;
+    F2M_CUDA(cudaMemcpyAsync(&db, B.dmin_bits + b, sizeof(db), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    H.V = V;
+    std::memcpy(&H.dmin, &db, sizeof(double));
+    std::vector<int64_t> row;
+    if (d2h(ctx, row, B.row + base, V + 1)) return F2M_ERR_CUDA;
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    const int64_t s0 = row[0], S = row[V] - row[0];
+    H.row.resize(V + 1);
+    for (int v = 0; v <= V; ++v) H.row[v] = row[v] - s0;
+    std::vector<Slot> sl;
+    std::vector<int> em, oth;
+    f2m_status s = F2M_OK;
+    if ((s = d2h(ctx, sl, B.slot + s0, S))) return s;
+    if ((s = d2h(ctx, H.cost, B.s_cost + s0, S))) return s;
+    if ((s = d2h(ctx, H.perm, B.perm + s0, S))) return s;
+    if ((s = d2h(ctx, H.mirror, B.mirror + s0, S))) return s;
+    if ((s = d2h(ctx, H.F, B.F + base, V))) return s;
+    if ((s = d2h(ctx, H.efcnt, B.efcnt + base, V))) return s;
+    if ((s = d2h(ctx, H.ccnt, B.ccnt + base, V))) return s;
+    if ((s = d2h(ctx, H.label, B.K + base, V))) return s;
+    if (with_keys) {
+        if ((s = d2h(ctx, em, B.s_em + s0, S))) return s;
+        if ((s = d2h(ctx, oth, B.s_oth + s0, S))) return s;
+    }
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    H.nbr.resize(S);
+    H.Dn.resize(S);
+    for (int64_t a = 0; a < S; ++a) { H.nbr[a] = sl[a].nbr; H.Dn[a] = sl[a].D; }
+    if (with_keys) {
+        // keys hold FXY indices; node ids here are the same indices
+        number_edges(H, em, oth);
+    }
+    return F2M_OK;
+}
+
+// graph::RUN after the descent (graph_cuda.cu:64-153) for one instance:
+// host comb check, repair loop through device refits, primal and report values.
+f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& prm, f2m_result& R) {
+    HostInst& H = R.H;
+    const double vb = prm.error_B * prm.error_B_comb;
+    HostCheck HC(H, vb);
+    int IRR_B = HC.check();
+    int steps = 0;
+    if (IRR_B > 0) {
+        int64_t ibase = 0, s0 = 0;
+        F2M_CUDA(cudaMemcpyAsync(&ibase, C.B.offs + b, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+        F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+        F2M_CUDA(cudaMemcpyAsync(&s0, C.B.row + ibase, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+        F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+        double sv = prm.shift0;
+        std::vector<double> sh;
+        const int32_t one = b;
+        // cuda_IRREGULAR_B_recompute + get_combs_cuda + host_combs_check
+        auto step = [&](double shiftV, int type) -> int {
+            steps++;
+            HC.shifts(shiftV, type, sh);
+            Batch B = C.B;
+            B.n_items = 1;
+            const int32_t st = kNeedsHost;
+            cudaError_t e;
+            if ((e = cudaMemcpyAsync(const_cast<double*>(B.shift) + ibase, sh.data(), sh.size() * sizeof(double),
+                                     cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(C.ord, &one, sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(B.status + b, &st, sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+                (e = launch_refit(B, to_dev(prm), C.vcap, C.threads, ctx->stream, &ctx->launches)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(H.F.data(), B.F + ibase, H.V * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(H.efcnt.data(), B.efcnt + ibase, H.V * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(H.ccnt.data(), B.ccnt + ibase, H.V * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(H.perm.data(), B.perm + s0, H.perm.size() * sizeof(uint16_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess) {
+                ctx->err = cudaGetErrorString(e);
+                return -1;
+            }
+            int32_t st2 = 0;
+            cudaMemcpyAsync(&st2, B.status + b, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+            if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) { ctx->err = cudaGetErrorString(e); return -1; }
+            if (st2 == F2M_ERR_NOT_CONVERGED || st2 == F2M_ERR_CAPACITY) return -2;
+            return HC.check();
+        };
+        for (;;) {  // graph_cuda.cu:74-126
+            if ((IRR_B = step(sv, 0)) <= 0) break;
+            if ((IRR_B = step(sv, 1)) <= 0) break;
+            sv = -sv;
+            if ((IRR_B = step(sv, 0)) <= 0) break;
+            sv = -sv;
+            if ((IRR_B = step(sv, 1)) <= 0) break;
+            sv = -sv;
+            sv *= 2;
+            if (std::fabs(sv) > prm.shift_max) break;
+        }
+        if (IRR_B == -1) return fail(ctx, F2M_ERR_CUDA, "repair step failed: " + ctx->err);
+        if (IRR_B == -2) IRR_B = 1;
+    }
+    R.st.repair_steps = steps;
+    R.st.irr_a = HC.irr_a;
+    R.st.irr_b = IRR_B > 0 ? IRR_B : 0;
+    R.st.n_combs = (int32_t)HC.comb_V.size();
+    R.x.assign(H.E, 0.0);
+    R.X.clear();
+    if (IRR_B == 0) {
+        for (int v = 0; v < H.V; ++v)  // node::get_eA_X (node.cpp:61-71)
+            for (int e : HC.eA[v]) {
+                const int v0 = H.label[v];
+                if (v0 < H.label[H.el1[e]]) R.X[e] = 1;
+                if (v0 < H.label[H.el2[e]]) R.X[e] = 1;
+            }
+        for (auto& Cb : HC.Combs)
+            for (auto& kv : Cb.XB) R.X[kv.first] = kv.second;
+        double OVAL = 0;  // graph::getOVAL (graph_tour.hpp:165-184)
+        int mr = 0;
+        for (auto& kv : R.X) {
+            const int e = kv.first;
+            mr = std::max(mr, std::min(H.rank1[e], H.rank2[e]));
+            OVAL += kv.second * H.eDo[e];
+            R.x[e] = kv.second;
+        }
+        R.lp = OVAL;
+        R.max_rank = mr;
+        R.status = F2M_OK;
+        // graph::check_solution (graph_tour.hpp:142-163)
+        std::vector<float> deg(H.V, 0.0f);
+        std::vector<char> has(H.V, 0);
+        for (auto& kv : R.X) {
+            deg[H.el1[kv.first]] += (float)kv.second; has[H.el1[kv.first]] = 1;
+            deg[H.el2[kv.first]] += (float)kv.second; has[H.el2[kv.first]] = 1;
+        }
+        int viol = 0;
+        for (int v = 0; v < H.V; ++v)
+            if (has[v] && !(deg[v] > 2.0f - 1e-2f && deg[v] < 2.0f + 1e-2f)) viol++;
+        R.st.degree_violations = viol;
+    } else {
+        R.status = F2M_ERR_NOT_CONVERGED;
+        R.err = "Optimal Solution not Found";
+        R.lp = NAN;
+    }
+    // FP64 dual bound with u = -F/2 in d_min units
+    double fsum = 0, neg = 0;
+    for (int v = 0; v < H.V; ++v) fsum += H.F[v];
+    for (int e = 0; e < H.E; ++e) {
+        const double d = (H.eD[e] + 0.5 * H.F[H.ev1[e]]) + 0.5 * H.F[H.ev2[e]];
+        neg += std::min(0.0, d);
+    }
+    R.st.dual_value = H.dmin * (-fsum + neg);
+    R.st.d_min = H.dmin;
+    return F2M_OK;
+}
+
+f2m_status pull_stats(f2m_ctx* ctx, const DevCall& C, int b, f2m_result& R) {
+    int64_t it = 0;
+    int32_t ch = 0;
+    double mg = 0;
+    F2M_CUDA(cudaMemcpyAsync(&it, C.B.iters + b, sizeof(it), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(&ch, C.B.checks + b, sizeof(ch), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(&mg, C.B.max_grad + b, sizeof(mg), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    R.st.iterations = it;
+    R.st.checks = ch;
+    R.st.max_grad = mg;
+    return F2M_OK;
+}
+
+}  // namespace
+
+/* ------------------------------------------------------------------ */
+/* C ABI                                                                */
+/* ------------------------------------------------------------------ */
+extern "C" {
+
+void f2m_default_params(f2m_params* p) {
+    p->error_B = 1e-7;
+    p->error_B_comb = 1e2;
+    p->glob_K = 5;
+    p->glob_rounds = 200;
+    p->glob_inner = 50;
+    p->glob_tol = 0.01;
+    p->factor0 = 100;
+    p->factor_step = 300;
+    p->factor_cap = 5000;
+    p->max_rounds = 10000;
+    p->fix_rounds = 100;
+    p->fix_factor = 500;
+    p->check_every = 50;
+    p->frozen_iters = 20;
+    p->ef_thr = 1.0;
+    p->ef_small_deg = 10;
+    p->ef_min = 3;
+    p->comb_thr = 0.25;
+    p->shift0 = 0.5;
+    p->shift_max = 32;
+    p->max_iters = 20000000;
+    p->cost_mode = F2M_COST_REF_EUCLID;
+    p->threads = 0;
+}
+
+f2m_status f2m_create(f2m_ctx** out, int device) {
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return F2M_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) return F2M_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return F2M_ERR_NO_DEVICE;
+    f2m_ctx* c = new f2m_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return F2M_ERR_CUDA;
+    }
+    for (auto& e : c->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            delete c;
+            return F2M_ERR_CUDA;
+        }
+    *out = c;
+    return F2M_OK;
+}
+
+void f2m_destroy(f2m_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->dev) cudaFree(c->dev);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+f2m_status f2m_phase_times(f2m_ctx* ctx, float* ms, f2m_work* work) {
+    if (!ctx || !ctx->timed) return F2M_ERR_INPUT;
+    F2M_CUDA(cudaEventSynchronize(ctx->ev[4]));
+    for (int k = 0; k < 4; ++k) F2M_CUDA(cudaEventElapsedTime(ms + k, ctx->ev[k], ctx->ev[k + 1]));
+    if (work) {
+        const Batch& B = ctx->last;
+        const int n = B.n_inst;
+        std::vector<int64_t> wn(n), ws(n);
+        std::vector<int32_t> vn(n), st(n);
+        int64_t slots = 0;
+        F2M_CUDA(cudaMemcpy(wn.data(), B.work_nodes, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(ws.data(), B.work_slots, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(vn.data(), B.Vn, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(&slots, B.row + B.n_total, sizeof(int64_t), cudaMemcpyDeviceToHost));
+        *work = f2m_work{0, 0, slots, 0};
+        for (int b = 0; b < n; ++b) {
+            work->node_iters += wn[b];
+            work->slot_iters += ws[b];
+            work->points += vn[b];
+        }
+    }
+    return F2M_OK;
+}
+
+const char* f2m_last_error(const f2m_ctx* c) { return c ? c->err.c_str() : "no context"; }
+int64_t f2m_kernel_launches(const f2m_ctx* c) { return c ? c->launches : 0; }
+
+f2m_status f2m_sync(f2m_ctx* ctx) {
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    return F2M_OK;
+}
+
+static f2m_status check_args(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, int32_t top_k,
+                             const f2m_params* params) {
+    if (!ctx) return F2M_ERR_INPUT;
+    if (n_inst < 1 || !offs) return fail(ctx, F2M_ERR_INPUT, "need at least one instance");
+    if (top_k < 3) return fail(ctx, F2M_ERR_INPUT, "N must be at least 3");
+    if (top_k > 256) return fail(ctx, F2M_ERR_CAPACITY, "N above 256 is not supported");
+    if (params && params->cost_mode != F2M_COST_REF_EUCLID)
+        return fail(ctx, F2M_ERR_INPUT, "only the reference cost mode runs on the device");
+    for (int32_t b = 0; b < n_inst; ++b)
+        if (offs[b + 1] < offs[b]) return fail(ctx, F2M_ERR_INPUT, "offsets must be non-decreasing");
+    if (offs[0] != 0) return fail(ctx, F2M_ERR_INPUT, "offs[0] must be 0");
+    if (offs[n_inst] > INT32_MAX) return fail(ctx, F2M_ERR_CAPACITY, "too many points in one call");
+    return F2M_OK;
+}
+
+// Host completion of the batch instances whose combs need the Ax=b stage.
+static f2m_status complete_batch(f2m_ctx* ctx, DevCall& C, const f2m_params& prm,
+                                 std::vector<int32_t>& status, std::vector<double>& lp,
+                                 std::vector<int32_t>* max_rank) {
+    for (int b = 0; b < C.pl.n_inst; ++b) {
+        if (status[b] != kNeedsHost) continue;
+        f2m_result R;
+        f2m_status s = pull_instance(ctx, C, b, R.H, true);
+        if (s) return s;
+        if ((s = complete_instance(ctx, C, b, prm, R))) return s;
+        status[b] = R.status;
+        lp[b] = R.lp;
+        if (max_rank) (*max_rank)[b] = R.max_rank;
+    }
+    return F2M_OK;
+}
+
+f2m_status f2m_solve_batch(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const double* x,
+                           const double* y, int32_t top_k, const f2m_params* params,
+                           f2m_batch_out* out) {
+    f2m_status s = check_args(ctx, n_inst, offs, top_k, params);
+    if (s) return s;
+    if (!out || !out->lp || !out->status) return fail(ctx, F2M_ERR_INPUT, "lp and status outputs are required");
+    f2m_params prm;
+    f2m_default_params(&prm);
+    if (params) prm = *params;
+    cudaSetDevice(ctx->device);
+    DevCall C;
+    if ((s = setup_call(ctx, C, n_inst, offs, top_k, prm, true))) return s;
+    const int64_t n = C.pl.n_total;
+    F2M_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(C.B.offs), offs, (n_inst + 1) * sizeof(int64_t),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.X_in), x, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.Y_in), y, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if ((s = run_device(ctx, C, prm, true, true))) return s;
+    std::vector<int32_t> status(n_inst), mr;
+    std::vector<double> lp(n_inst);
+    F2M_CUDA(cudaMemcpyAsync(status.data(), C.B.status, n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(lp.data(), C.B.lp, n_inst * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (out->max_rank) {
+        mr.resize(n_inst);
+        F2M_CUDA(cudaMemcpyAsync(mr.data(), C.B.max_rank, n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (out->n_nodes) F2M_CUDA(cudaMemcpyAsync(out->n_nodes, C.B.Vn, n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    if (out->n_edges) F2M_CUDA(cudaMemcpyAsync(out->n_edges, C.B.n_edges, n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    if (out->n_combs) F2M_CUDA(cudaMemcpyAsync(out->n_combs, C.B.n_combs, n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    if (out->iterations) F2M_CUDA(cudaMemcpyAsync(out->iterations, C.B.iters, n_inst * sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if ((s = complete_batch(ctx, C, prm, status, lp, out->max_rank ? &mr : nullptr))) return s;
+    std::memcpy(out->status, status.data(), n_inst * sizeof(int32_t));
+    std::memcpy(out->lp, lp.data(), n_inst * sizeof(double));
+    if (out->max_rank) std::memcpy(out->max_rank, mr.data(), n_inst * sizeof(int32_t));
+    return F2M_OK;
+}
+
+f2m_status f2m_solve_batch_device(f2m_ctx* ctx, int32_t n_inst, const int64_t* h_offs,
+                                  const int64_t* d_offs, const double* d_x, const double* d_y,
+                                  int32_t top_k, const f2m_params* params, f2m_batch_out* d_out) {
+    f2m_status s = check_args(ctx, n_inst, h_offs, top_k, params);
+    if (s) return s;
+    if (!d_out || !d_out->lp || !d_out->status) return fail(ctx, F2M_ERR_INPUT, "lp and status outputs are required");
+    f2m_params prm;
+    f2m_default_params(&prm);
+    if (params) prm = *params;
+    cudaSetDevice(ctx->device);
+    DevCall C;
+    if ((s = setup_call(ctx, C, n_inst, h_offs, top_k, prm, false))) return s;
+    C.B.offs = d_offs;
+    C.B.X_in = d_x;
+    C.B.Y_in = d_y;
+    if ((s = run_device(ctx, C, prm, true, true))) return s;
+    // instances whose combs need the host Ax=b stage are completed here
+    std::vector<int32_t> status(n_inst);
+    F2M_CUDA(cudaMemcpyAsync(status.data(), C.B.status, n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    bool any = false;
+    for (int32_t v : status) any |= (v == kNeedsHost);
+    if (any) {
+        std::vector<double> lp;
+        if ((s = d2h(ctx, lp, C.B.lp, n_inst))) return s;
+        F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+        if ((s = complete_batch(ctx, C, prm, status, lp, nullptr))) return s;
+        F2M_CUDA(cudaMemcpyAsync(C.B.lp, lp.data(), n_inst * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        F2M_CUDA(cudaMemcpyAsync(C.B.status, status.data(), n_inst * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+        F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+        return dst ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream) : cudaSuccess;
+    };
+    F2M_CUDA(cp(d_out->lp, C.B.lp, n_inst * sizeof(double)));
+    F2M_CUDA(cp(d_out->status, C.B.status, n_inst * sizeof(int32_t)));
+    F2M_CUDA(cp(d_out->n_nodes, C.B.Vn, n_inst * sizeof(int32_t)));
+    F2M_CUDA(cp(d_out->n_edges, C.B.n_edges, n_inst * sizeof(int32_t)));
+    F2M_CUDA(cp(d_out->n_combs, C.B.n_combs, n_inst * sizeof(int32_t)));
+    F2M_CUDA(cp(d_out->max_rank, C.B.max_rank, n_inst * sizeof(int32_t)));
+    F2M_CUDA(cp(d_out->iterations, C.B.iters, n_inst * sizeof(int64_t)));
+    return F2M_OK;
+}
+
+f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels,
+                            int32_t n, int32_t top_k, const f2m_params* params, f2m_result** out) {
+    *out = nullptr;
+    const int64_t offs[2] = {0, n};
+    f2m_status s = check_args(ctx, 1, offs, top_k, params);
+    if (s) return s;
+    f2m_params prm;
+    f2m_default_params(&prm);
+    if (params) prm = *params;
+    cudaSetDevice(ctx->device);
+    std::unique_ptr<f2m_result> R(new f2m_result());
+    DevCall C;
+    if ((s = setup_call(ctx, C, 1, offs, top_k, prm, true))) return s;
+    int32_t* dK = nullptr;
+    if (labels) {
+        // labels ride in the (unused) cursor buffer until k_prep compacts them
+        dK = C.B.cursor;
+        C.B.K_in = dK;
+        F2M_CUDA(cudaMemcpyAsync(dK, labels, n * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    F2M_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(C.B.offs), offs, 2 * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.X_in), x, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.Y_in), y, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    auto t0 = std::chrono::steady_clock::now();
+    F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
+    F2M_CUDA(launch_knn(C.B, ctx->stream, &ctx->launches));
+    C.B.K_in = nullptr;
+    F2M_CUDA(launch_graph(C.B, C.deg, C.scan, ctx->stream, &ctx->launches));
+    F2M_CUDA(launch_solve(C.B, to_dev(prm), C.vcap, C.threads, ctx->stream, &ctx->launches));
+    int32_t st = 0;
+    F2M_CUDA(cudaMemcpyAsync(&st, C.B.status, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (st != F2M_OK && st != kNeedsHost) {
+        R->status = st;
+        R->err = st == F2M_ERR_INPUT ? "invalid instance (fewer than 4 distinct points or degenerate box)"
+                                     : "instance exceeds a solver limit or did not converge";
+        *out = R.release();
+        return (f2m_status)st;
+    }
+    if ((s = pull_instance(ctx, C, 0, R->H, true))) return s;
+    if ((s = pull_stats(ctx, C, 0, *R))) return s;
+    if ((s = complete_instance(ctx, C, 0, prm, *R))) return s;
+    if ((s = pull_stats(ctx, C, 0, *R))) return s;
+    R->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = R.release();
+    return (f2m_status)(*out)->status;
+}
+
+
+}  // extern "C"
+
+namespace {
+
+/* ------------------------------------------------------------------ */
+/* TSPLIB input (FXY.hpp:186-309) on the host                           */
+/* ------------------------------------------------------------------ */
+struct FilePoints {
+    std::vector<int> K;
+    std::vector<double> X, Y;
+    // duplicates[k0][k] (FXY.hpp:37,263)
+    std::unordered_map<int, std::unordered_map<int, int>> duplicates;
+};
+
+f2m_status parse_tsplib(const std::string& path, FilePoints& P, std::string& err) {
+    std::ifstream F(path);
+    if (!F.is_open()) { err = "cannot open " + path; return F2M_ERR_INPUT; }
+    std::string line, body;
+    int start = 0, count = 0;
+    while (std::getline(F, line)) {  // get_size (FXY.hpp:186-229)
+        if (line.compare(0, 3, "EOF") == 0) break;
+        if (start == 1) { count++; body += line; body += ' '; continue; }
+        if (line.compare(0, 18, "NODE_COORD_SECTION") == 0) start = 1;
+    }
+    if (count == 0) { err = "file " + path + " is not in TSPLIB format"; return F2M_ERR_INPUT; }
+    std::unordered_map<double, std::unordered_map<double, int>> filtr;  // FXY.hpp:233
+    const char* p = body.c_str();
+    for (;;) {  // get_KXY (FXY.hpp:241-291)
+        int k = -1, n = 0;
+        double x = 0, y = 0;
+        int r = sscanf(p, "%d%n", &k, &n);
+        if (r == EOF) break;
+        if (r != 1) { err = "non-numeric token in NODE_COORD_SECTION"; return F2M_ERR_INPUT; }
+        p += n;
+        if (sscanf(p, "%lf%n", &x, &n) != 1) { err = "truncated coordinate triple"; return F2M_ERR_INPUT; }
+        p += n;
+        if (sscanf(p, "%lf%n", &y, &n) != 1) { err = "truncated coordinate triple"; return F2M_ERR_INPUT; }
+        p += n;
+        x = std::round(x * 1000);
+        y = std::round(y * 1000);
+        x /= 1000;
+        y /= 1000;
+        if (k <= -1) continue;
+        auto fx = filtr.find(x);
+        if (fx != filtr.end()) {
+            auto fy = fx->second.find(y);
+            if (fy != fx->second.end()) { P.duplicates[fy->second][k]++; continue; }
+        }
+        filtr[x][y] = k;
+        P.K.push_back(k);
+        P.X.push_back(x);
+        P.Y.push_back(y);
+    }
+    return F2M_OK;
+}
+
+// One kNN list entry as the device produced it (FXY index space).
+struct TopE {
+    double cost;
+    int em, oth, a, b;  // key (cost, em, oth); endpoints a<b
+};
+bool top_less(const TopE& x, const TopE& y) {
+    if (x.cost != y.cost) return x.cost < y.cost;
+    if (x.em != y.em) return x.em < y.em;
+    return x.oth < y.oth;
+}
+
+// graph::graph (graph_tour.hpp:28-110) + graph_c::init (graph_cuda_init.hpp:3-70):
+// kept edges in global order, nodes created in order of first appearance,
+// internal ids in unordered_map<int,node*> iteration order.
+void assemble_ref(const FilePoints& P, const std::vector<TopE>& kept, HostInst& H,
+                  std::vector<int>& fxy_of) {
+    const int n = (int)P.X.size();
+    std::unordered_map<int, int> map_node;
+    for (const TopE& e : kept) {
+        const int ks[2] = {e.a, e.b};
+        for (int f : ks)
+            if (map_node.count(P.K[f]) == 0) map_node[P.K[f]] = f;
+    }
+    std::vector<int> id_of(n, -1);
+    int iV = 0;
+    fxy_of.clear();
+    for (auto& kv : map_node) { id_of[kv.second] = iV++; fxy_of.push_back(kv.second); }
+    H.V = iV;
+    H.label.resize(iV);
+    for (int v = 0; v < iV; ++v) H.label[v] = P.K[fxy_of[v]];
+    H.E = (int)kept.size();
+    H.ev1.resize(H.E); H.ev2.resize(H.E); H.el1.resize(H.E); H.el2.resize(H.E);
+    H.rank1.resize(H.E); H.rank2.resize(H.E); H.eD.resize(H.E); H.eDo.resize(H.E);
+    double dmin = 1e16;
+    for (int e = 0; e < H.E; ++e) {
+        const int u = id_of[kept[e].a], v = id_of[kept[e].b];
+        H.ev1[e] = std::min(u, v); H.ev2[e] = std::max(u, v);
+        if (H.label[u] < H.label[v]) { H.el1[e] = u; H.el2[e] = v; }
+        else { H.el1[e] = v; H.el2[e] = u; }
+        H.eDo[e] = kept[e].cost;
+        dmin = std::min(dmin, kept[e].cost);
+    }
+    H.dmin = dmin;
+    for (int e = 0; e < H.E; ++e) H.eD[e] = H.eDo[e] / dmin;
+    H.row.assign(H.V + 1, 0);
+    for (int e = 0; e < H.E; ++e) { H.row[H.ev1[e] + 1]++; H.row[H.ev2[e] + 1]++; }
+    for (int v = 0; v < H.V; ++v) H.row[v + 1] += H.row[v];
+    const int64_t S = H.row[H.V];
+    H.nbr.assign(S, 0); H.Dn.assign(S, 0); H.cost.assign(S, 0); H.perm.assign(S, 0);
+    H.mirror.assign(S, 0); H.slot_edge.assign(S, 0);
+    std::vector<int64_t> fill(H.row.begin(), H.row.end() - 1);
+    for (int e = 0; e < H.E; ++e) {
+        const int u = H.ev1[e], v = H.ev2[e];
+        const int64_t su = fill[u]++, sv = fill[v]++;
+        H.nbr[su] = v; H.nbr[sv] = u;
+        H.Dn[su] = H.Dn[sv] = H.eD[e];
+        H.cost[su] = H.cost[sv] = H.eDo[e];
+        H.slot_edge[su] = H.slot_edge[sv] = e;
+        const int ru = (int)(su - H.row[u]), rv = (int)(sv - H.row[v]);
+        H.perm[su] = (uint16_t)ru; H.perm[sv] = (uint16_t)rv;
+        H.mirror[su] = rv; H.mirror[sv] = ru;
+        if (H.el1[e] == u) { H.rank1[e] = ru; H.rank2[e] = rv; }
+        else { H.rank1[e] = rv; H.rank2[e] = ru; }
+    }
+}
+
+void write_outputs(const std::string& file, int top_k, const FilePoints& P, const std::vector<TopE>& dm,
+                   const f2m_result& R) {
+    const std::string base = file + ".top" + std::to_string(top_k);
+    {   // FXY::save_to_file (FXY.hpp:146-165)
+        std::ofstream f(base + ".DM");
+        std::unordered_map<int, int> stat;
+        for (const TopE& e : dm) {
+            if (stat[e.a] > top_k && stat[e.b] > top_k) continue;
+            stat[e.a]++;
+            stat[e.b]++;
+            f << e.a << " " << e.b << " " << e.cost << "\n";
+        }
+    }
+    if (!P.duplicates.empty()) {  // FXY::save_to_file_duplicates (FXY.hpp:168-183)
+        std::ofstream f(file + "_duplicates");
+        for (auto& kv : P.duplicates) {
+            f << "node used: " << kv.first << " duplicates: ";
+            for (auto& kk : kv.second) f << kk.first << " ";
+            f << "\n";
+        }
+    }
+    {   // graph::print_file_report (graph_tour.hpp:218-241)
+        std::ofstream f(base + ".F2M_report");
+        if (R.status == F2M_OK) {
+            f << "Optimal Found: " << "Yes" << "\n";
+            f << "Optimal Value: " << std::setprecision(15) << R.lp << "\n";
+            f << "Time: " << R.seconds << "\n";
+            f << "MAX edge rank: " << R.max_rank << "\n";
+        } else {
+            f << "ERROR: Optimal Solution not Found\n";
+        }
+    }
+    if (R.status == F2M_OK) {  // graph::print_file_solution (graph_tour.hpp:186-214)
+        std::ofstream f(base + ".F2M_solution");
+        for (auto& kv : R.X) {
+            const int e = kv.first;
+            f << R.H.label[R.H.el1[e]] << " " << R.H.label[R.H.el2[e]] << " " << std::setprecision(4)
+              << kv.second << "\n";
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k, const f2m_params* params,
+                          int32_t write_files, f2m_result** out) {
+    *out = nullptr;
+    if (!ctx) return F2M_ERR_INPUT;
+    if (!path) return fail(ctx, F2M_ERR_INPUT, "no file");
+    f2m_params prm;
+    f2m_default_params(&prm);
+    if (params) prm = *params;
+    FilePoints FP;
+    std::string err;
+    f2m_status s = parse_tsplib(path, FP, err);
+    if (s) return fail(ctx, s, err);
+    const int32_t n = (int32_t)FP.X.size();
+    const int64_t offs[2] = {0, n};
+    if ((s = check_args(ctx, 1, offs, top_k, params))) return s;
+    if (n < 4) return fail(ctx, F2M_ERR_INPUT, "fewer than 4 distinct points");
+    cudaSetDevice(ctx->device);
+    std::unique_ptr<f2m_result> R(new f2m_result());
+    // kNN on the device with N+1 per node: the first N build the graph, all
+    // N+1 give the .DM file (its cap is N+1 per node, FXY.hpp:156)
+    const int32_t N1 = std::min(top_k + 1, 256);
+    DevCall C;
+    if ((s = setup_call(ctx, C, 1, offs, N1, prm, true))) return s;
+    C.B.N_cut = top_k;
+    int32_t* dK = C.B.cursor;
+    C.B.K_in = dK;
+    F2M_CUDA(cudaMemcpyAsync(dK, FP.K.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(C.B.offs), offs, 2 * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.X_in), FP.X.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.Y_in), FP.Y.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
+    F2M_CUDA(launch_knn(C.B, ctx->stream, &ctx->launches));
+    C.B.K_in = nullptr;
+    int32_t st = 0;
+    F2M_CUDA(cudaMemcpyAsync(&st, C.B.status, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<int32_t> ntop, tn, tem, toth;
+    std::vector<double> tc;
+    if ((s = d2h(ctx, ntop, C.B.ntop, n)) || (s = d2h(ctx, tn, C.B.top_nbr, (size_t)n * N1)) ||
+        (s = d2h(ctx, tc, C.B.top_cost, (size_t)n * N1)) || (s = d2h(ctx, tem, C.B.top_em, (size_t)n * N1)) ||
+        (s = d2h(ctx, toth, C.B.top_oth, (size_t)n * N1)))
+        return s;
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (st != F2M_OK) return fail(ctx, (f2m_status)st, "invalid instance (degenerate bounding box)");
+    // union of the first N (graph) and first N+1 (.DM) of every node's list
+    std::vector<TopE> kept, dm;
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < ntop[i]; ++k) {
+            const int64_t o = (int64_t)i * N1 + k;
+            const int j = tn[o];
+            TopE e{tc[o], tem[o], toth[o], std::min(i, j), std::max(i, j)};
+            dm.push_back(e);
+            if (k < top_k) kept.push_back(e);
+        }
+    auto dedup = [](std::vector<TopE>& v) {
+        std::sort(v.begin(), v.end(), top_less);
+        size_t w = 0;
+        for (size_t r = 0; r < v.size(); ++r)
+            if (w == 0 || v[r].a != v[w - 1].a || v[r].b != v[w - 1].b || v[r].cost != v[w - 1].cost) v[w++] = v[r];
+        v.resize(w);
+    };
+    dedup(kept);
+    dedup(dm);
+    HostInst& H = R->H;
+    std::vector<int> fxy_of;
+    assemble_ref(FP, kept, H, fxy_of);
+    // upload the graph in the reference's node order as instance 0
+    {
+        std::vector<int64_t> row(H.row.begin(), H.row.end());
+        std::vector<Slot> sl(H.nbr.size());
+        for (size_t a = 0; a < sl.size(); ++a) {
+            sl[a].D = H.Dn[a];
+            sl[a].nbr = H.nbr[a];
+            sl[a].aux = H.perm[a];
+        }
+        const int32_t Vn = H.V, ok = F2M_OK;
+        unsigned long long db;
+        std::memcpy(&db, &H.dmin, sizeof(db));
+        if ((s = h2d(ctx, C.B.row, row)) || (s = h2d(ctx, C.B.slot, sl)) || (s = h2d(ctx, C.B.s_cost, H.cost)) ||
+            (s = h2d(ctx, C.B.perm, H.perm)) || (s = h2d(ctx, C.B.mirror, H.mirror)))
+            return s;
+        F2M_CUDA(cudaMemcpyAsync(C.B.Vn, &Vn, sizeof(Vn), cudaMemcpyHostToDevice, ctx->stream));
+        F2M_CUDA(cudaMemcpyAsync(C.B.status, &ok, sizeof(ok), cudaMemcpyHostToDevice, ctx->stream));
+        F2M_CUDA(cudaMemcpyAsync(C.B.dmin_bits, &db, sizeof(db), cudaMemcpyHostToDevice, ctx->stream));
+        F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    // graph::RUN (graph_cuda.cu:47-155), timed like dtimeRUN
+    auto t0 = std::chrono::steady_clock::now();
+    F2M_CUDA(launch_solve(C.B, to_dev(prm), C.vcap, C.threads, ctx->stream, &ctx->launches));
+    F2M_CUDA(cudaMemcpyAsync(&st, C.B.status, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (st != F2M_OK && st != kNeedsHost) return fail(ctx, (f2m_status)st, "the device solve stopped early");
+    if ((s = d2h(ctx, H.F, C.B.F, H.V)) || (s = d2h(ctx, H.efcnt, C.B.efcnt, H.V)) ||
+        (s = d2h(ctx, H.ccnt, C.B.ccnt, H.V)) || (s = d2h(ctx, H.perm, C.B.perm, H.nbr.size())))
+        return s;
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if ((s = pull_stats(ctx, C, 0, *R))) return s;
+    if ((s = complete_instance(ctx, C, 0, prm, *R))) return s;
+    R->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if ((s = pull_stats(ctx, C, 0, *R))) return s;
+    if (write_files) write_outputs(path, top_k, FP, dm, *R);
+    *out = R.release();
+    return (f2m_status)(*out)->status;
+}
+
+void f2m_result_free(f2m_result* r) { delete r; }
+int32_t f2m_result_status(const f2m_result* r) { return r->status; }
+int32_t f2m_result_n_nodes(const f2m_result* r) { return r->H.V; }
+int32_t f2m_result_n_edges(const f2m_result* r) { return r->H.E; }
+double f2m_result_lp(const f2m_result* r) { return r->lp; }
+int32_t f2m_result_max_rank(const f2m_result* r) { return r->max_rank; }
+double f2m_result_seconds(const f2m_result* r) { return r->seconds; }
+
+void f2m_result_edges(const f2m_result* r, int32_t* v1, int32_t* v2, int32_t* lab1, int32_t* lab2,
+                      double* Do, double* D, double* x) {
+    const HostInst& H = r->H;
+    for (int e = 0; e < H.E; ++e) {
+        if (v1) v1[e] = H.ev1[e];
+        if (v2) v2[e] = H.ev2[e];
+        if (lab1) lab1[e] = H.label[H.el1[e]];
+        if (lab2) lab2[e] = H.label[H.el2[e]];
+        if (Do) Do[e] = H.eDo[e];
+        if (D) D[e] = H.eD[e];
+        if (x) x[e] = e < (int)r->x.size() ? r->x[e] : 0.0;
+    }
+}
+void f2m_result_nodes(const f2m_result* r, int32_t* label, double* F) {
+    for (int v = 0; v < r->H.V; ++v) {
+        if (label) label[v] = r->H.label[v];
+        if (F) F[v] = r->H.F[v];
+    }
+}
+void f2m_result_stats(const f2m_result* r, f2m_stats* s) { *s = r->st; }
+
+}  // extern "C"

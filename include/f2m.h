@@ -1,0 +1,183 @@
+/*
+ * f2m_b200 -- C ABI of the B200-native F2M (fractional 2-matching) solver.
+ *
+ * Plain pointers and sizes only; no torch or CUDA types cross this boundary.
+ * Every entry point returns an f2m_status; nothing calls exit().  Host arrays
+ * belong to the caller; device buffers belong to the context.  One context
+ * per host thread (a context owns one CUDA stream on one device).
+ *
+ * Each entry point names the reference interface it replaces
+ * (aav-antonov/F2M, paths relative to that project).
+ */
+#ifndef F2M_B200_H
+#define F2M_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum f2m_status {
+    F2M_OK = 0,
+    F2M_ERR_INPUT = 1,          /* bad file/arguments (reference: exit(0), FXY.hpp:221-226) */
+    F2M_ERR_CAPACITY = 2,       /* instance exceeds a compiled limit */
+    F2M_ERR_NOT_CONVERGED = 3,  /* "ERROR: Optimal Solution not Found" (graph_tour.hpp:236-239) */
+    F2M_ERR_CUDA = 4,           /* a CUDA call failed (reference: cudaCheckErrors exit(1)) */
+    F2M_ERR_NO_DEVICE = 5       /* no CUDA device / the kernels are not loadable */
+} f2m_status;
+
+typedef enum f2m_cost_mode {
+    F2M_COST_REF_EUCLID = 0,    /* raw FP64 sqrt(dx^2+dy^2), as FXY.hpp:382 */
+    F2M_COST_NINT = 1           /* TSPLIB EUC_2D nint(); oracle-only for now */
+} f2m_cost_mode;
+
+/* The reference's hard-coded constants, now parameters (defaults equal the
+ * reference; graph_cuda.cu:56-57,178-186,214-216,370-394,
+ * graph_cuda_partition.hpp:50,62, graph_cuda_comb.hpp:420,556). */
+typedef struct f2m_params {
+    double error_B;        /* 1e-7: convergence on max|grad| */
+    double error_B_comb;   /* 1e2: half-edge band = error_B * error_B_comb */
+    int32_t glob_K;        /* 5 */
+    int32_t glob_rounds;   /* 200 */
+    int32_t glob_inner;    /* 50 */
+    double glob_tol;       /* 0.01 */
+    int32_t factor0;       /* 100 */
+    int32_t factor_step;   /* 300 */
+    int32_t factor_cap;    /* 5000 */
+    int32_t max_rounds;    /* 10000 */
+    int32_t fix_rounds;    /* 100 */
+    int32_t fix_factor;    /* 500 */
+    int32_t check_every;   /* 50 */
+    int32_t frozen_iters;  /* 20 */
+    double ef_thr;         /* 1.0 */
+    int32_t ef_small_deg;  /* 10 */
+    int32_t ef_min;        /* 3 */
+    double comb_thr;       /* 0.25 */
+    double shift0;         /* 0.5 */
+    double shift_max;      /* 32 */
+    int64_t max_iters;     /* safety cap on Jacobi iterations per solve (not in the reference) */
+    int32_t cost_mode;     /* f2m_cost_mode */
+    int32_t threads;       /* CTA width of the batched solver; 0 = autotuned */
+} f2m_params;
+
+typedef struct f2m_ctx f2m_ctx;
+
+/* Fill *p with the reference's constants. */
+void f2m_default_params(f2m_params* p);
+
+/* Create a context on `device`.  Replaces the implicit CUDA context set-up of
+ * graph_c::init_cuda (graph_cuda_init.hpp:102-193). */
+f2m_status f2m_create(f2m_ctx** ctx, int device);
+void f2m_destroy(f2m_ctx* ctx);
+/* Last error message of this context (never NULL). */
+const char* f2m_last_error(const f2m_ctx* ctx);
+/* Kernels launched by this context since creation (diagnostics). */
+int64_t f2m_kernel_launches(const f2m_ctx* ctx);
+
+/* ------------------------------------------------------------------ */
+/* Batched solve: many independent instances in one call.               */
+/* The reference solves one file per process (RUN.cpp:12-31); this entry  */
+/* is its batched replacement: per instance it runs FXY (FXY.hpp:23-144), */
+/* the union-of-kNN graph build (graph_tour.hpp:28-98), the descent       */
+/* (graph_cuda.cu:163-430), comb extraction (graph_cuda_comb.hpp:415-475) */
+/* and the host comb check + primal (graph_cuda_comb.hpp:121-147,         */
+/* graph_cuda.cu:135-147) and returns the report's Optimal Value.         */
+/* ------------------------------------------------------------------ */
+typedef struct f2m_batch_out {
+    double* lp;            /* [n_inst] Optimal Value (sum x*Do); NaN when not found */
+    int32_t* status;       /* [n_inst] f2m_status per instance */
+    int32_t* n_nodes;      /* optional [n_inst]: nodes after de-duplication */
+    int32_t* n_edges;      /* optional [n_inst] */
+    int32_t* n_combs;      /* optional [n_inst] */
+    int32_t* max_rank;     /* optional [n_inst] "MAX edge rank" */
+    int64_t* iterations;   /* optional [n_inst] Jacobi iterations */
+} f2m_batch_out;
+
+/* Host arrays: offs[n_inst+1] (int64) into x[], y[] (FP64 coordinates,
+ * rounded to 1e-3 and de-duplicated as get_KXY does, FXY.hpp:252-267). */
+f2m_status f2m_solve_batch(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs,
+                           const double* x, const double* y, int32_t top_k,
+                           const f2m_params* params, f2m_batch_out* out);
+
+/* Same, with offs/x/y already resident in device memory (d_ pointers); the
+ * host copy h_offs plans the launch.  Outputs are device pointers too (lp,
+ * status required; others optional), written on the context stream; the
+ * call returns once they are enqueued (f2m_sync() waits for them). */
+f2m_status f2m_solve_batch_device(f2m_ctx* ctx, int32_t n_inst, const int64_t* h_offs,
+                                  const int64_t* d_offs, const double* d_x, const double* d_y,
+                                  int32_t top_k, const f2m_params* params,
+                                  f2m_batch_out* d_out);
+f2m_status f2m_sync(f2m_ctx* ctx);
+
+/* Work counters of the last batched call, summed over its instances. */
+typedef struct f2m_work {
+    int64_t node_iters;    /* sum over Jacobi iterations of the nodes updated */
+    int64_t slot_iters;    /* sum over Jacobi iterations of the active slots read */
+    int64_t slots;         /* CSR slots built (2 x edges) */
+    int64_t points;        /* points after de-duplication */
+} f2m_work;
+
+/* Device time (CUDA events on the context stream) of the phases of the last
+ * batched call: ms[0] rounding/de-duplication, ms[1] kNN, ms[2] graph build,
+ * ms[3] the persistent solver (descent, combs, primal).  Diagnostics; no
+ * reference counterpart (the reference prints gettimeofday phase times,
+ * graph_cuda_define.hpp:29-34). */
+f2m_status f2m_phase_times(f2m_ctx* ctx, float* ms, f2m_work* work);
+
+/* ------------------------------------------------------------------ */
+/* Single instance with full results (the F2M.h graph API).             */
+/* ------------------------------------------------------------------ */
+typedef struct f2m_result f2m_result;
+
+/* Points in (labels optional: NULL = 1..n).  Node ids follow the
+ * de-duplicated input order.  Replaces graph(file,N) + graph_c + RUN()
+ * (F2M.h:181,320,175) for in-memory inputs. */
+f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y,
+                            const int32_t* labels, int32_t n, int32_t top_k,
+                            const f2m_params* params, f2m_result** out);
+
+/* `F2M.solver.exe file N` (RUN.cpp:12-31): parse the TSPLIB file, solve, and
+ * when write_files != 0 write <file>.topN.F2M_report / .F2M_solution
+ * (graph_tour.hpp:186-241), .DM (FXY.hpp:146-165) and <file>_duplicates
+ * (FXY.hpp:168-183).  Node ids follow the reference's graph order
+ * (graph_tour.hpp:95-97). */
+f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k,
+                          const f2m_params* params, int32_t write_files,
+                          f2m_result** out);
+
+void f2m_result_free(f2m_result* r);
+int32_t f2m_result_status(const f2m_result* r);
+int32_t f2m_result_n_nodes(const f2m_result* r);
+int32_t f2m_result_n_edges(const f2m_result* r);
+/* graph::OVAL and graph::MAXrankDo (graph_tour.hpp:165-184) */
+double f2m_result_lp(const f2m_result* r);
+int32_t f2m_result_max_rank(const f2m_result* r);
+/* Seconds spent in the solve proper (the report's "Time:", graph_cuda.cu:51,131). */
+double f2m_result_seconds(const f2m_result* r);
+/* Edges in the graph's edge order: internal node ids (v1<v2), TSPLIB labels
+ * of the lower/higher-label endpoint, raw cost Do, normalised cost D and the
+ * primal value x (graph::X, F2M.h:161; 0 where absent).  Any pointer may be
+ * NULL. */
+void f2m_result_edges(const f2m_result* r, int32_t* v1, int32_t* v2, int32_t* lab1,
+                      int32_t* lab2, double* Do, double* D, double* x);
+/* Per node: TSPLIB label, dual potential F (graph::F, F2M.h:146). */
+void f2m_result_nodes(const f2m_result* r, int32_t* label, double* F);
+
+typedef struct f2m_stats {
+    int64_t iterations;    /* all Jacobi iterations */
+    int32_t checks;        /* check_OPT calls */
+    int32_t n_combs;
+    int32_t irr_a;         /* combs failing 2A+B=4 at the final check */
+    int32_t irr_b;         /* combs whose Ax=b did not converge */
+    int32_t repair_steps;
+    int32_t degree_violations; /* nodes with |sum x - 2| >= 1e-2 (graph_tour.hpp:142-163) */
+    double max_grad;       /* max|grad| at the last check */
+    double d_min;
+    double dual_value;     /* FP64 dual bound 2*sum(u) + sum(min(0,d)) with u=-F/2 */
+} f2m_stats;
+void f2m_result_stats(const f2m_result* r, f2m_stats* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,155 @@
+"""CUDA path vs the CPU oracle (parity), through the C ABI.
+
+Node ids, edge order and every FP64 expression follow the reference, so the
+device potentials F must equal the oracle's bit for bit, the kNN edge list
+must be identical, and the LP value must agree to rounding (the device sums
+sum(x*Do) in a different order: tolerance 1e-12 relative, well inside the
+1e-9 target)."""
+import os
+
+import numpy as np
+import pytest
+
+import f2m_b200
+from f2m_b200 import synth
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+LP_RTOL = 1e-12
+
+
+def _close(a, b, rtol=LP_RTOL):
+    return abs(a - b) <= rtol * max(abs(a), abs(b))
+
+
+def _check_against(r, ref_status, ref_lp, ref_max_rank, lab1, lab2, Do, F, xval):
+    assert r.status == ref_status
+    assert np.array_equal(r.lab1, lab1), "kNN edge list differs"
+    assert np.array_equal(r.lab2, lab2)
+    assert np.array_equal(r.Do, Do)
+    assert np.array_equal(r.F, F), "potentials differ from the oracle"
+    if ref_status == 0:
+        assert _close(r.lp, ref_lp)
+        assert r.max_rank == ref_max_rank
+        assert np.array_equal(r.x, xval)
+
+
+@pytest.mark.parametrize("name", ["uniform200_n10", "config1_n20", "lattice150_s1_n8",
+                                  "lattice150_s3_n8"])
+def test_points_match_golden(ctx, name):
+    g = np.load(os.path.join(GOLDEN, f"oracle_{name}.npz"))
+    r = ctx.solve_points(g["x"], g["y"], int(g["N"]))
+    _check_against(r, int(g["status"]), float(g["lp"]), int(g["max_rank"]), g["lab1"], g["lab2"],
+                   g["Do"], g["F"], g["xval"])
+
+
+def test_file_path_matches_golden_reference_order(ctx, tmp_path):
+    """`F2M.solver.exe file N`: reference node order, report and solution files."""
+    g = np.load(os.path.join(GOLDEN, "oracle_config1_ref_n20.npz"))
+    path = str(tmp_path / "c1.tsp")
+    synth.write_tsplib(path, g["x"], g["y"])
+    r = ctx.solve_file(path, 20, write_files=True)
+    _check_against(r, int(g["status"]), float(g["lp"]), int(g["max_rank"]), g["lab1"], g["lab2"],
+                   g["Do"], g["F"], g["xval"])
+    assert np.array_equal(r.label, g["node_label"])
+    rep = open(path + ".top20.F2M_report").read().splitlines()
+    assert rep[0] == "Optimal Found: Yes"
+    assert rep[1] == "Optimal Value: %.15g" % r.lp
+    assert rep[3] == "MAX edge rank: %d" % int(g["max_rank"])
+    sol = [ln.split() for ln in open(path + ".top20.F2M_solution")]
+    got = {(int(a), int(b)): float(c) for a, b, c in sol}
+    want = {(int(a), int(b)): float(c) for a, b, c in zip(g["lab1"], g["lab2"], g["xval"]) if c}
+    assert got == want
+    assert os.path.exists(path + ".top20.DM")
+
+
+def test_points_vs_oracle_live(ctx, oracle):
+    """Fresh seeds: the oracle is run here next to the device."""
+    for seed, n, N in [(21, 120, 6), (22, 777, 12), (23, 2500, 16), (24, 5000, 16)]:
+        x, y = synth.uniform_int_points(n, seed)
+        o = oracle.solve_points(x, y, N)
+        r = ctx.solve_points(x, y, N)
+        _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+
+
+def test_lattice_repair_vs_oracle(ctx, oracle):
+    """Many equal distances: tie order of the kNN and the comb repair loop."""
+    for seed in (2, 4, 7, 11):
+        x, y = synth.lattice_points(300, seed)
+        o = oracle.solve_points(x, y, 8)
+        r = ctx.solve_points(x, y, 8)
+        _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+        assert r.stats["repair_steps"] == o.stats["repair_steps"]
+
+
+def test_duplicates_and_rounding(ctx, oracle):
+    """get_KXY drops repeated points after 1e-3 rounding (FXY.hpp:252-267)."""
+    x, y = synth.uniform_int_points(400, 31)
+    x = np.concatenate([x, x[:40] + 0.0004])
+    y = np.concatenate([y, y[:40]])
+    frac = synth.uniform(31, 9, len(x)) * 0.01
+    x = x + frac
+    o = oracle.solve_points(x, y, 10)
+    r = ctx.solve_points(x, y, 10)
+    assert r.n_nodes == o.n_nodes < len(x)
+    _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+
+
+def test_batch_matches_oracle(ctx, oracle):
+    offs, x, y = synth.config3(seed=5, n_inst=40, hi=1500)
+    # two lattice instances go through the host comb stage
+    lx, ly = synth.lattice_points(150, 1)
+    lx2, ly2 = synth.lattice_points(150, 3)
+    x = np.concatenate([x, lx, lx2])
+    y = np.concatenate([y, ly, ly2])
+    offs = np.concatenate([offs, [offs[-1] + 150, offs[-1] + 300]])
+    out = ctx.solve_batch(offs, x, y, 16, details=True)
+    lp_o, st_o, _ = oracle.solve_batch(offs, x, y, 16, threads=os.cpu_count() or 1)
+    assert np.array_equal(out["status"], st_o)
+    ok = st_o == 0
+    assert np.all(np.abs(out["lp"][ok] - lp_o[ok]) <= LP_RTOL * np.abs(lp_o[ok]))
+
+
+def test_batch_equals_plain_path(ctx):
+    """Batched LP values equal the per-instance (plain) path."""
+    offs, x, y = synth.config3(seed=6, n_inst=16, hi=900)
+    lp, st = ctx.solve_batch(offs, x, y, 16)
+    for b in range(16):
+        r = ctx.solve_points(x[offs[b]:offs[b + 1]], y[offs[b]:offs[b + 1]], 16)
+        assert r.status == st[b]
+        assert _close(r.lp, lp[b])
+
+
+def test_primal_is_feasible_and_gap_closed(ctx):
+    x, y = synth.config1(8)
+    r = ctx.solve_points(x, y, 20)
+    assert r.status == 0
+    deg = np.zeros(r.n_nodes)
+    np.add.at(deg, r.v1, r.x)
+    np.add.at(deg, r.v2, r.x)
+    assert np.allclose(deg, 2.0)
+    assert set(np.unique(r.x)).issubset({0.0, 0.5, 1.0})
+    assert r.stats["degree_violations"] == 0
+    assert abs(r.stats["dual_value"] - r.lp) <= 1e-9 * r.lp
+    assert r.stats["max_grad"] < 1e-7
+
+
+def test_input_errors(ctx):
+    with pytest.raises(f2m_b200.F2MError) as e:
+        ctx.solve_points(np.array([0.0, 1, 2]), np.array([0.0, 1, 5]), 3)
+    assert e.value.status == f2m_b200.ERR_INPUT
+    with pytest.raises(f2m_b200.F2MError) as e:
+        ctx.solve_points(*synth.uniform_int_points(50, 1), 2)
+    assert e.value.status == f2m_b200.ERR_INPUT
+    with pytest.raises(f2m_b200.F2MError):
+        ctx.solve_file("/nonexistent/file.tsp", 10)
+
+
+def test_zero_x_span_is_solved(ctx, oracle):
+    """A vertical line of points: the reference's ring radius is 0 and its
+    stat pass never ends (FXY.hpp:305,528); here the y-span takes over."""
+    y = np.arange(60, dtype=np.float64) * 3.0 + synth.uniform(3, 1, 60).round(3)
+    x = np.zeros(60)
+    o = oracle.solve_points(x, y, 6)
+    r = ctx.solve_points(x, y, 6)
+    _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
