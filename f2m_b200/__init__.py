@@ -241,6 +241,8 @@ class Context:
         if not h:
             raise F2MError(s, self.last_error())
         try:
+            if s not in (OK, ERR_NOT_CONVERGED):
+                raise F2MError(s, self.last_error() or "invalid instance")
             return Result(h)
         finally:
             lib().f2m_result_free(h)
