@@ -72,7 +72,8 @@ struct Batch {
     Slot* slot;             // [S]
     uint16_t* perm;         // [S] per-node list order (local positions)
     int32_t* mirror;        // [S] position of the same edge in the neighbour's list
-    Slot* ef;               // [S] active-set arena (update_EF copies)
+    double* efD;            // [S] active-set arena (update_EF copies): D
+    uint16_t* efN;          // [S] active-set arena: neighbour
     uint8_t* xcode;         // [S] 0, 1 (= 1/2), 2 (= 1)
     int64_t S_cap;
     // per-node state kept between the solve and the host comb check
@@ -107,17 +108,20 @@ cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches);
 cudaError_t launch_knn(const Batch& B, cudaStream_t s, int64_t* launches);
 cudaError_t launch_graph(const Batch& B, int64_t* deg_scratch, int64_t* scan_scratch,
                          cudaStream_t s, int64_t* launches);
-cudaError_t launch_solve(const Batch& B, const DevParams& P, int32_t v_max, int threads,
-                         cudaStream_t s, int64_t* launches);
-// Repair step for the instances listed in B.order[0..B.n_items): F += shift,
-// frozen iterations, run_fix, comb partition (graph_cuda_comb.hpp:542-574).
-cudaError_t launch_refit(const Batch& B, const DevParams& P, int32_t v_max, int threads,
-                         cudaStream_t s, int64_t* launches);
+// Persistent solver over items[0..n_items) of size class c (largest first);
+// queue is a device counter.  REFIT variant: F += shift, frozen iterations,
+// run_fix (graph_cuda_comb.hpp:542-574).
+cudaError_t launch_solve_class(int c, const Batch& B, const DevParams& P, const int32_t* items,
+                               int n_items, int32_t* queue, int vcap, cudaStream_t s,
+                               int64_t* launches);
+cudaError_t launch_refit_class(int c, const Batch& B, const DevParams& P, const int32_t* items,
+                               int n_items, int32_t* queue, int vcap, cudaStream_t s,
+                               int64_t* launches);
+int solve_num_classes();
+int solve_class_of(int32_t n);
 cudaError_t launch_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* scratch,
                         cudaStream_t s, int64_t* launches);
 int64_t scan_scratch_elems(int64_t n);
-int solve_blocks_per_sm(int threads, size_t smem);
-size_t solve_smem_bytes(int32_t v_max);
 int32_t solve_max_nodes();
 
 }  // namespace f2m

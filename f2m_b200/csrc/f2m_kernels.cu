@@ -608,174 +608,312 @@ cudaError_t launch_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* scr
 }
 
 /* ------------------------------------------------------------------ */
-/* the solver: one CTA runs one instance's whole schedule               */
+/* the solver: a team of threads runs one instance's whole schedule      */
 /* ------------------------------------------------------------------ */
+// A CTA holds TEAMS independent teams of TEAM threads.  Each team takes
+// instances from a work counter and keeps, per instance, the potentials F
+// (double-buffered for the Jacobi step), the EF offsets and the EF lists
+// (D as FP64, neighbour as u16) in its slice of shared memory; EF lists that
+// do not fit spill to a global arena at the same offsets.  Team barriers are
+// named barriers (bar.sync id, TEAM).
+template <int TEAM>
+struct Team {
+    int tid, id;
+    double* sred;       // TEAM/32
+    long long* sredl;   // TEAM/32
+    int* swarp;         // TEAM/32 + 1
+    int* sint;          // 4 ints
+    __device__ __forceinline__ void sync() const {
+        asm volatile("bar.sync %0, %1;" ::"r"(id + 1), "r"(TEAM) : "memory");
+    }
+    __device__ double max(double x) const {
+        const int lane = tid & 31, w = tid >> 5;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0) sred[w] = x;
+        sync();
+        double r = -INFINITY;
+        for (int k = 0; k < TEAM / 32; ++k) r = fmax(r, sred[k]);
+        sync();
+        return r;
+    }
+    __device__ double sum(double x) const {
+        const int lane = tid & 31, w = tid >> 5;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sred[w] = x;
+        sync();
+        double r = 0.0;
+        for (int k = 0; k < TEAM / 32; ++k) r += sred[k];  // same order in every thread
+        sync();
+        return r;
+    }
+    __device__ long long sum_ll(long long x) const {
+        const int lane = tid & 31, w = tid >> 5;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sredl[w] = x;
+        sync();
+        long long r = 0;
+        for (int k = 0; k < TEAM / 32; ++k) r += sredl[k];
+        sync();
+        return r;
+    }
+    __device__ long long max_ll(long long x) const {
+        const int lane = tid & 31, w = tid >> 5;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = ::max(x, (long long)__shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0) sredl[w] = x;
+        sync();
+        long long r = LLONG_MIN;
+        for (int k = 0; k < TEAM / 32; ++k) r = ::max(r, sredl[k]);
+        sync();
+        return r;
+    }
+    // exclusive scan in team-thread order; *total = team sum
+    __device__ int excl_scan(int x, int* total) const {
+        const int lane = tid & 31, w = tid >> 5;
+        int inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) swarp[w] = inc;
+        sync();
+        int before = 0, tot = 0;
+        for (int k = 0; k < TEAM / 32; ++k) {
+            const int v = swarp[k];
+            if (k < w) before += v;
+            tot += v;
+        }
+        sync();
+        *total = tot;
+        return before + inc - x;
+    }
+};
+
 struct Inst {
     int V;
     int64_t base;          // first node index
     const int64_t* row;    // row[v], v in [0, V]
     const Slot* slot;
     uint16_t* perm;
-    Slot* ef;              // EF arena of this instance (starts at row[0])
+    double* gD;            // global EF arena of this instance (D)
+    uint16_t* gN;          // (neighbour)
 };
 
-// Reduced cost of a slot of node v: D + 0.5*F[v1] + 0.5*F[v2] with v1<v2
-// (cuda_recompute_Edges, graph_cuda_grad.hpp:257-268).
-__device__ __forceinline__ double red_d(const Slot& s, int v, const double* F, double fv) {
-    const double fn = F[s.nbr];
-    return (v < s.nbr) ? (s.D + 0.5 * fv) + 0.5 * fn : (s.D + 0.5 * fn) + 0.5 * fv;
+// Shared-memory slice of one team.  H = F/2 is kept instead of F: halving is
+// exact, so H_new = H + grad/2 equals F_new/2 bit for bit and a reduced cost
+// D + 0.5*F[v1] + 0.5*F[v2] is (D + H[v1]) + H[v2] with the same rounding.
+struct TeamMem {
+    double* Ha;
+    double* Hb;
+    int* efo;        // V+1
+    double* eD;      // cap
+    uint16_t* eW;    // cap: neighbour id | 0x8000 when the neighbour is the lower id
+    int cap;
+};
+
+__device__ __forceinline__ TeamMem carve_team(unsigned char* base, size_t bytes, int vcap) {
+    TeamMem M;
+    M.Ha = reinterpret_cast<double*>(base);
+    M.Hb = M.Ha + vcap;
+    M.efo = reinterpret_cast<int*>(M.Hb + vcap);
+    const size_t used = (size_t)vcap * 16 + (((size_t)vcap + 1) * 4 + 7) / 8 * 8;
+    M.eD = reinterpret_cast<double*>(base + used);
+    const long long rest = (long long)bytes - (long long)used;
+    int cap = rest > 0 ? (int)(rest / 10) : 0;
+    cap &= ~7;
+    M.eW = reinterpret_cast<uint16_t*>(M.eD + cap);
+    M.cap = cap;
+    return M;
 }
 
-// cuda_get_Nodes_grad_R (graph_cuda_grad.hpp:321-340) over a node's EF list.
-__device__ __forceinline__ double ef_grad(const Inst& I, const int* efo, const double* F, int v) {
-    const int o0 = efo[v], n = efo[v + 1] - o0;
-    const double fv = F[v];
-    const Slot* e = I.ef + o0;
-    double v0 = red_d(e[0], v, F, fv), v1 = 1e6, v2 = 1e6;
+__device__ __forceinline__ uint16_t ef_word(int v, int nbr) {
+    return (uint16_t)(nbr | (nbr < v ? 0x8000 : 0));
+}
+
+// Reduced cost of a slot of node v: D + 0.5*F[v1] + 0.5*F[v2] with v1<v2
+// (cuda_recompute_Edges, graph_cuda_grad.hpp:257-268), from H = F/2.
+__device__ __forceinline__ double red_d(const Slot& s, int v, const double* H, double hv) {
+    const double hn = H[s.nbr];
+    return (v < s.nbr) ? (s.D + hv) + hn : (s.D + hn) + hv;
+}
+
+// cuda_get_Nodes_grad_R (graph_cuda_grad.hpp:321-340) over a node's EF list:
+// the 2nd and 3rd smallest of {first, rest.., 1e6, 1e6}.  While the first
+// value is below 1e6 the reference's compare chain keeps v0<=v1<=v2 and is a
+// sorted insertion, done here by a branch-free min/max network; otherwise the
+// chain itself runs (it can then leave v0 > v1).  Returns grad/2 = -(v1+v2)/4,
+// the step of H.
+__device__ __forceinline__ void top3_insert(double x, double& v0, double& v1, double& v2) {
+    const double t = fmax(v0, x);
+    v0 = fmin(v0, x);
+    const double u = fmax(v1, t);
+    v1 = fmin(v1, t);
+    v2 = fmin(v2, u);
+}
+__device__ __forceinline__ double ef_half_grad(const double* __restrict__ Dp,
+                                               const uint16_t* __restrict__ Wp, int n, double hv,
+                                               const double* __restrict__ H) {
+    auto dv = [&](int k) {
+        const uint16_t w = Wp[k];
+        const double a = H[w & 0x7fff];
+        const bool lo = (w & 0x8000) != 0;
+        return (Dp[k] + (lo ? a : hv)) + (lo ? hv : a);
+    };
+    double v0 = dv(0), v1 = 1e6, v2 = 1e6;
+    if (n >= 3) {
+        const double x1 = dv(1), x2 = dv(2);
+        if (v0 < 1e6) {
+            top3_insert(x1, v0, v1, v2);
+            top3_insert(x2, v0, v1, v2);
+            for (int k = 3; k < n; ++k) top3_insert(dv(k), v0, v1, v2);
+            return (-(v1 + v2) / 2) * 0.5;
+        }
+    }
     for (int k = 1; k < n; ++k) {
-        const double x = red_d(e[k], v, F, fv);
+        const double x = dv(k);
         if (x < v0) { v2 = v1; v1 = v0; v0 = x; continue; }
         if (x < v1) { v2 = v1; v1 = x; continue; }
         if (x < v2) { v2 = x; }
     }
-    return -(v1 + v2) / 2;
+    return (-(v1 + v2) / 2) * 0.5;
 }
 
 __device__ __forceinline__ double pdv(const Inst& I, int64_t r0, const uint16_t* list, int k, int v,
-                                      const double* F, double fv) {
-    return red_d(I.slot[r0 + list[k]], v, F, fv);
+                                      const double* H, double hv) {
+    return red_d(I.slot[r0 + list[k]], v, H, hv);
 }
 
 // qpart_ptr_B (graph_cuda_partition.hpp:3-25), the bound tested first.  On
 // finite values it performs at most size/2 swaps; the pass cap only matters
 // for NaN values (where the reference loops forever) and keeps the kernel
 // finite.
-__device__ int qpart_b(const Inst& I, int64_t r0, int v, const double* F, int size, double avg) {
+__device__ int qpart_b(const Inst& I, int64_t r0, int v, const double* H, int size, double avg) {
     uint16_t* list = I.perm + r0;
-    const double fv = F[v];
+    const double hv = H[v];
     int low = 0, high = size - 1, i = low, j = high;
     for (int pass = 0; i < j && pass <= size; ++pass) {
-        while (i <= high && pdv(I, r0, list, i, v, F, fv) <= avg) i++;
-        while (j >= low && pdv(I, r0, list, j, v, F, fv) > avg) j--;
+        while (i <= high && pdv(I, r0, list, i, v, H, hv) <= avg) i++;
+        while (j >= low && pdv(I, r0, list, j, v, H, hv) > avg) j--;
         if (i < j) { const uint16_t t = list[i]; list[i] = list[j]; list[j] = t; }
     }
     return j + 1;
 }
 // qpart_ptr_EF (graph_cuda_partition.hpp:27-54): raise the threshold by 1
 // until at least ef_min entries qualify (bounded: see qpart_b).
-__device__ int qpart_ef(const Inst& I, int64_t r0, int v, const double* F, int size, double avg,
+__device__ int qpart_ef(const Inst& I, int64_t r0, int v, const double* H, int size, double avg,
                         int ef_min) {
     if (size < ef_min) return size;  // the reference would not terminate
     for (int bump = 0; bump < (1 << 20); ++bump) {
-        const int p = qpart_b(I, r0, v, F, size, avg);
+        const int p = qpart_b(I, r0, v, H, size, avg);
         if (p >= ef_min) return p;
         avg += 1;
     }
     return size;
 }
 
-template <int T>
-struct Cta {
-    double* sred;
-    int* swarp;
-    int* s_carry;
-    long long* sredl;
-
-    // efo[0..V) holds counts -> exclusive offsets, efo[V] = total
-    __device__ void scan_counts(int* efo, int V) const {
-        if (threadIdx.x == 0) *s_carry = 0;
-        __syncthreads();
-        for (int r = 0; r < V; r += T) {
-            const int v = r + threadIdx.x;
-            const int c = (v < V) ? efo[v] : 0;
-            int tot;
-            const int ex = block_excl_scan<T>(c, swarp, &tot);
-            if (v < V) efo[v] = *s_carry + ex;
-            __syncthreads();
-            if (threadIdx.x == 0) *s_carry += tot;
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) efo[V] = *s_carry;
-        __syncthreads();
-    }
-    // update_EF (graph_cuda.cu:229-252): copy each node's list prefix
-    __device__ void rebuild_ef(const Inst& I, const int* efo) const {
-        for (int v = threadIdx.x; v < I.V; v += T) {
-            const int64_t r0 = I.row[v];
-            const int o0 = efo[v], n = efo[v + 1] - o0;
-            for (int k = 0; k < n; ++k) I.ef[o0 + k] = I.slot[r0 + I.perm[r0 + k]];
-        }
-        __syncthreads();
-    }
-    __device__ double grad_max(const Inst& I, const int* efo, const double* F) const {
-        double m = 0.0;
-        for (int v = threadIdx.x; v < I.V; v += T) m = fmax(m, fabs(ef_grad(I, efo, F, v)));
-        return block_max<T>(m, sred);
-    }
-    // one Jacobi step: Fn = Fc + grad(Fc)
-    __device__ void jacobi(const Inst& I, const int* efo, const double* Fc, double* Fn) const {
-        for (int v = threadIdx.x; v < I.V; v += T) Fn[v] = Fc[v] + ef_grad(I, efo, Fc, v);
-        __syncthreads();
-    }
-};
-
-// Per-instance solver state in shared memory: two F buffers (Jacobi double
-// buffering) and the EF offsets efo[0..V].
-template <int T>
+template <int TEAM>
 struct Solver {
     const Batch& B;
     const DevParams& P;
     const Inst& I;
-    const Cta<T>& C;
-    double* Fc;
-    double* Fn;
-    int* efo;
+    const Team<TEAM>& T;
+    TeamMem M;
+    double* Hc;   // H = F/2, current
+    double* Hn;   // next (Jacobi double buffer)
     long long iters = 0;
-    long long wslots = 0;  // active slots read, summed over iterations (thread 0)
+    long long wslots = 0;  // active slots read, summed over iterations
     int checks = 0;
     bool capped = false;
 
-    __device__ Solver(const Batch& b, const DevParams& p, const Inst& i, const Cta<T>& c, double* fa,
-                      double* fb, int* e)
-        : B(b), P(p), I(i), C(c), Fc(fa), Fn(fb), efo(e) {}
+    __device__ Solver(const Batch& b, const DevParams& p, const Inst& i, const Team<TEAM>& t, TeamMem m)
+        : B(b), P(p), I(i), T(t), M(m), Hc(m.Ha), Hn(m.Hb) {}
 
     __device__ int deg(int v) const { return (int)(I.row[v + 1] - I.row[v]); }
-    __device__ void swap_f() { double* t = Fc; Fc = Fn; Fn = t; }
+    __device__ void swap_f() { double* t = Hc; Hc = Hn; Hn = t; }
+    // grad/2 of node v over its EF list
+    __device__ __forceinline__ double hgrad(int v) const {
+        const int o = M.efo[v], n = M.efo[v + 1] - o;
+        const bool sm = o + n <= M.cap;
+        return ef_half_grad(sm ? M.eD + o : I.gD + o, sm ? M.eW + o : I.gN + o, n, Hc[v], Hc);
+    }
+    // one Jacobi step: F += grad(F) (graph_cuda.cu:293-304), as H += grad/2
     __device__ void jacobi() {
-        if (threadIdx.x == 0) wslots += efo[I.V];
-        C.jacobi(I, efo, Fc, Fn);
+        for (int v = T.tid; v < I.V; v += TEAM) Hn[v] = Hc[v] + hgrad(v);
+        wslots += M.efo[I.V];
+        T.sync();
         swap_f();
         iters++;
     }
     // block_EF_iter_BLOCK (graph_cuda.cu:278-289): frozen nodes keep F
     __device__ void jacobi_masked() {
-        for (int v = threadIdx.x; v < I.V; v += T) {
-            const double g = ef_grad(I, efo, Fc, v);
-            Fn[v] = (B.shift[I.base + v] != 0.0) ? Fc[v] : Fc[v] + g;
+        for (int v = T.tid; v < I.V; v += TEAM) {
+            const double g = hgrad(v);
+            Hn[v] = (B.shift[I.base + v] != 0.0) ? Hc[v] : Hc[v] + g;
         }
-        if (threadIdx.x == 0) wslots += efo[I.V];
-        __syncthreads();
+        wslots += M.efo[I.V];
+        T.sync();
         swap_f();
         iters++;
     }
+    // max |grad| (max_node_grad, graph_cuda_maxmin.hpp:29-37)
+    __device__ double grad_max() const {
+        double m = 0.0;
+        for (int v = T.tid; v < I.V; v += TEAM) m = fmax(m, fabs(hgrad(v)));
+        return 2.0 * T.max(m);
+    }
+    // efo[0..V) counts -> exclusive offsets (node order), efo[V] = total
+    __device__ void scan_counts() {
+        int* efo = M.efo;
+        int carry = 0;
+        for (int r = 0; r < I.V; r += TEAM) {
+            const int v = r + T.tid;
+            const int c = (v < I.V) ? efo[v] : 0;
+            int tot;
+            const int ex = T.excl_scan(c, &tot);
+            if (v < I.V) efo[v] = carry + ex;
+            carry += tot;
+        }
+        if (T.tid == 0) efo[I.V] = carry;
+        T.sync();
+    }
+    // update_EF (graph_cuda.cu:229-252): copy each node's list prefix
+    __device__ void rebuild_ef() {
+        for (int v = T.tid; v < I.V; v += TEAM) {
+            const int64_t r0 = I.row[v];
+            const int o = M.efo[v], n = M.efo[v + 1] - o;
+            const bool sm = o + n <= M.cap;
+            double* dD = sm ? M.eD + o : I.gD + o;
+            uint16_t* dW = sm ? M.eW + o : I.gN + o;
+            for (int k = 0; k < n; ++k) {
+                const Slot s = I.slot[r0 + I.perm[r0 + k]];
+                dD[k] = s.D;
+                dW[k] = ef_word(v, s.nbr);
+            }
+        }
+        T.sync();
+    }
     __device__ void finish_partition() {
-        __syncthreads();
-        C.scan_counts(efo, I.V);
-        C.rebuild_ef(I, efo);
+        T.sync();
+        scan_counts();
+        rebuild_ef();
     }
     // check_OPT + update_EF (graph_cuda.cu:229-271) with cuda_partition_v2
     __device__ double check_opt() {
-        for (int v = threadIdx.x; v < I.V; v += T) {
+        for (int v = T.tid; v < I.V; v += TEAM) {
             const int d = deg(v);
-            efo[v] = (d < P.ef_small_deg) ? d : qpart_ef(I, I.row[v], v, Fc, d, P.ef_thr, P.ef_min);
+            M.efo[v] = (d < P.ef_small_deg) ? d : qpart_ef(I, I.row[v], v, Hc, d, P.ef_thr, P.ef_min);
         }
         finish_partition();
         checks++;
-        return C.grad_max(I, efo, Fc);
+        return grad_max();
     }
     // block_EF (graph_cuda.cu:308-338)
     __device__ void block_ef(int N) {
-        const double MA = C.grad_max(I, efo, Fc);
+        const double MA = grad_max();
         int count_M = 0;
         for (int it = 0; it < N; ++it) {
             jacobi();
@@ -787,132 +925,158 @@ struct Solver {
     }
     // block_GLOB (graph_cuda.cu:363-430)
     __device__ void block_glob() {
-        for (int v = threadIdx.x; v < I.V; v += T) efo[v] = min(deg(v), P.glob_K);  // setvalue2V
+        for (int v = T.tid; v < I.V; v += TEAM) M.efo[v] = min(deg(v), P.glob_K);  // setvalue2V
         finish_partition();
         for (int go = 0; go < P.glob_rounds; ++go) {
             for (int it = 0; it < P.glob_inner; ++it) jacobi();
             // cuda_partition_v4 (graph_cuda_partition.hpp:89-115)
-            for (int v = threadIdx.x; v < I.V; v += T) {
+            for (int v = T.tid; v < I.V; v += TEAM) {
                 const int d = deg(v);
-                if (d < P.glob_K) { efo[v] = d; continue; }
+                if (d < P.glob_K) { M.efo[v] = d; continue; }
                 const int64_t r0 = I.row[v];
-                const double fv = Fc[v];
-                double avg = pdv(I, r0, I.perm + r0, 0, v, Fc, fv);
-                for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, I.perm + r0, k, v, Fc, fv));
-                efo[v] = qpart_ef(I, r0, v, Fc, d, avg, P.ef_min);
+                const double hv = Hc[v];
+                double avg = pdv(I, r0, I.perm + r0, 0, v, Hc, hv);
+                for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, I.perm + r0, k, v, Hc, hv));
+                M.efo[v] = qpart_ef(I, r0, v, Hc, d, avg, P.ef_min);
             }
             finish_partition();
-            if (C.grad_max(I, efo, Fc) < P.glob_tol) break;
+            if (grad_max() < P.glob_tol) break;
         }
     }
     // run_start_cuda (graph_cuda.cu:163-199)
     __device__ double run_start() {
         block_glob();
-        double M = check_opt();
+        double M_ = check_opt();
         int factor = P.factor0;
         for (int go = 1; go <= P.max_rounds; ++go) {
             block_ef(factor);
-            M = check_opt();
+            M_ = check_opt();
             if (factor < P.factor_cap) factor += P.factor_step;
-            if (M < P.error_B) break;
+            if (M_ < P.error_B) break;
             if (iters > P.max_iters) { capped = true; break; }
         }
-        return M;
+        return M_;
     }
     // run_fix_cuda (graph_cuda.cu:204-226)
     __device__ double run_fix() {
-        double M = check_opt();
+        double M_ = check_opt();
         for (int go = 1; go <= P.fix_rounds; ++go) {
             block_ef(P.fix_factor);
-            M = check_opt();
-            if (M < P.error_B) break;
+            M_ = check_opt();
+            if (M_ < P.error_B) break;
             if (iters > P.max_iters) { capped = true; break; }
         }
-        return M;
+        return M_;
+    }
+    // The EF lists in shared memory go to the global arena so that a later
+    // repair step (k_refit) resumes from exactly this update_EF state.
+    // Slots [0, smem_end()) belong to nodes whose whole list is in shared
+    // memory; a node straddling the capacity keeps its list in the arena.
+    __device__ int smem_end() const {
+        long long e = 0;
+        for (int v = T.tid; v <= I.V; v += TEAM)
+            if (M.efo[v] <= M.cap) e = ::max(e, (long long)M.efo[v]);
+        return (int)T.max_ll(e);
+    }
+    __device__ void spill_ef() {
+        const int n = smem_end();
+        for (int k = T.tid; k < n; k += TEAM) {
+            I.gD[k] = M.eD[k];
+            I.gN[k] = M.eW[k];
+        }
+    }
+    __device__ void load_ef() {
+        const int n = smem_end();
+        for (int k = T.tid; k < n; k += TEAM) {
+            M.eD[k] = I.gD[k];
+            M.eW[k] = I.gN[k];
+        }
+        T.sync();
     }
     // Comb extraction (graph_cuda_comb.hpp:415-475), the device comb check and
     // the primal; writes the per-node state for the host and the results.
-    __device__ void combs_and_primal(int b, double M, bool accumulate) {
+    __device__ void combs_and_primal(int b, double M_, bool accumulate) {
         const int V = I.V;
         const double porog = P.porog;
-        int* ccnt = reinterpret_cast<int*>(Fn);  // Fn is free: room for 2V ints
+        spill_ef();
+        int* ccnt = reinterpret_cast<int*>(Hn);  // Hn is free: room for 2V ints
         int* lab = ccnt + V;
-        for (int v = threadIdx.x; v < V; v += T)  // cuda_partition_v3
-            ccnt[v] = qpart_b(I, I.row[v], v, Fc, efo[v + 1] - efo[v], P.comb_thr);
-        __syncthreads();
-        for (int v = threadIdx.x; v < V; v += T) {
+        for (int v = T.tid; v < V; v += TEAM)  // cuda_partition_v3
+            ccnt[v] = qpart_b(I, I.row[v], v, Hc, M.efo[v + 1] - M.efo[v], P.comb_thr);
+        T.sync();
+        for (int v = T.tid; v < V; v += TEAM) {
             const int64_t r0 = I.row[v];
-            const double fv = Fc[v];
+            const double hv = Hc[v];
             bool has = false;
             for (int k = 0; k < ccnt[v] && !has; ++k) {
-                const double d = pdv(I, r0, I.perm + r0, k, v, Fc, fv);
+                const double d = pdv(I, r0, I.perm + r0, k, v, Hc, hv);
                 has = (d >= -porog && d <= porog);
             }
             lab[v] = has ? v : INT_MAX;
         }
-        __syncthreads();
+        T.sync();
         // a comb is a connected component of half edges rooted at its
         // smallest node id (get_cuda_comb_size, graph_cuda_comb.hpp:320-392);
         // min-label propagation over the half-edge frontier finds them
         volatile int* vlab = lab;
-        int changed;
-        do {
-            changed = 0;
-            for (int v = threadIdx.x; v < V; v += T) {
+        for (;;) {
+            int changed = 0;
+            for (int v = T.tid; v < V; v += TEAM) {
                 int m = vlab[v];
                 if (m == INT_MAX) continue;
                 const int64_t r0 = I.row[v];
-                const double fv = Fc[v];
+                const double hv = Hc[v];
                 for (int k = 0; k < ccnt[v]; ++k) {
                     const Slot s = I.slot[r0 + I.perm[r0 + k]];
-                    const double d = red_d(s, v, Fc, fv);
+                    const double d = red_d(s, v, Hc, hv);
                     if (d >= -porog && d <= porog) m = min(m, vlab[s.nbr]);
                 }
                 if (m < vlab[v]) { vlab[v] = m; changed = 1; }
             }
-        } while (__syncthreads_or(changed));
+            if (T.sum_ll(changed) == 0) break;
+        }
         // state for the host comb check
-        for (int v = threadIdx.x; v < V; v += T) {
-            B.F[I.base + v] = Fc[v];
-            B.efcnt[I.base + v] = efo[v + 1] - efo[v];
+        for (int v = T.tid; v < V; v += TEAM) {
+            B.F[I.base + v] = 2.0 * Hc[v];
+            B.efcnt[I.base + v] = M.efo[v + 1] - M.efo[v];
             B.ccnt[I.base + v] = ccnt[v];
         }
-        __syncthreads();
+        T.sync();
         // comb check (comb::solve_simple, comb_thread.cpp:180-195) with the
         // host's A/B rule (node::get_statusAB, node.cpp:49-57)
-        int* irr = efo;  // efo is no longer needed
-        for (int v = threadIdx.x; v < V; v += T) irr[v] = 0;
-        __syncthreads();
-        for (int v = threadIdx.x; v < V; v += T) {
+        int* irr = M.efo;  // efo is no longer needed
+        for (int v = T.tid; v < V; v += TEAM) irr[v] = 0;
+        T.sync();
+        for (int v = T.tid; v < V; v += TEAM) {
             if (lab[v] == INT_MAX) continue;
             const int64_t r0 = I.row[v], r1 = I.row[v + 1];
-            const double fv = Fc[v];
+            const double hv = Hc[v];
             int A = 0, Bc = 0;
             for (int64_t a = r0; a < r1; ++a) {
-                const double d = red_d(I.slot[a], v, Fc, fv);
+                const double d = red_d(I.slot[a], v, Hc, hv);
                 if (d < porog) { if (d > -porog) Bc++; else A++; }
             }
             if (4 - 2 * A - Bc != 0) irr[lab[v]] = 1;
         }
-        __syncthreads();
+        T.sync();
         long long nc = 0, ni = 0;
-        for (int v = threadIdx.x; v < V; v += T)
+        for (int v = T.tid; v < V; v += TEAM)
             if (lab[v] == v) { nc++; ni += irr[v]; }
-        nc = block_sum_ll<T>(nc, C.sredl);
-        ni = block_sum_ll<T>(ni, C.sredl);
+        nc = T.sum_ll(nc);
+        ni = T.sum_ll(ni);
         // primal (graph_cuda.cu:135-147): x = 1 on A edges, 1/2 on the B edges
         // of regular combs; OVAL = sum x*Do, MAX edge rank (graph_tour.hpp:165-184)
         double lp = 0.0, dual_neg = 0.0, fsum = 0.0;
         long long maxr = -1, viol = 0;
-        for (int v = threadIdx.x; v < V; v += T) {
+        for (int v = T.tid; v < V; v += TEAM) {
             const int64_t r0 = I.row[v], r1 = I.row[v + 1];
-            const double fv = Fc[v];
-            fsum += fv;
+            const double hv = Hc[v];
+            fsum += 2.0 * hv;
             float degsum = 0.0f;
             bool any = false;
             for (int64_t a = r0; a < r1; ++a) {
                 const Slot s = I.slot[a];
-                const double d = red_d(s, v, Fc, fv);
+                const double d = red_d(s, v, Hc, hv);
                 const double x = (d < porog) ? ((d > -porog) ? 0.5 : 1.0) : 0.0;
                 B.xcode[a] = (uint8_t)(x == 1.0 ? 2 : (x == 0.5 ? 1 : 0));
                 degsum += (float)x;
@@ -920,17 +1084,17 @@ struct Solver {
                 if (s.nbr > v) {
                     lp += x * B.s_cost[a];
                     dual_neg += fmin(0.0, d);
-                    if (x != 0.0) maxr = max(maxr, (long long)min((int)(a - r0), B.mirror[a]));
+                    if (x != 0.0) maxr = ::max(maxr, (long long)::min((int)(a - r0), B.mirror[a]));
                 }
             }
             if (any && !(degsum > 2.0f - 1e-2f && degsum < 2.0f + 1e-2f)) viol++;
         }
-        lp = block_sum<T>(lp, C.sred);
-        dual_neg = block_sum<T>(dual_neg, C.sred);
-        fsum = block_sum<T>(fsum, C.sred);
-        maxr = block_max_ll<T>(maxr, C.sredl);
-        viol = block_sum_ll<T>(viol, C.sredl);
-        if (threadIdx.x == 0) {
+        lp = T.sum(lp);
+        dual_neg = T.sum(dual_neg);
+        fsum = T.sum(fsum);
+        maxr = T.max_ll(maxr);
+        viol = T.sum_ll(viol);
+        if (T.tid == 0) {
             const double dmin = __longlong_as_double((long long)B.dmin_bits[b]);
             B.n_edges[b] = (int32_t)((I.row[V] - I.row[0]) / 2);
             B.n_combs[b] = (int32_t)nc;
@@ -941,13 +1105,13 @@ struct Solver {
             B.work_nodes[b] = (accumulate ? B.work_nodes[b] : 0) + iters * (long long)V;
             B.work_slots[b] = (accumulate ? B.work_slots[b] : 0) + wslots;
             B.checks[b] = (accumulate ? B.checks[b] : 0) + checks;
-            B.max_grad[b] = M;
+            B.max_grad[b] = M_;
             B.dual[b] = dmin * (-fsum + dual_neg);
             if (capped) { B.status[b] = F2M_ERR_NOT_CONVERGED; B.lp[b] = NAN; }
             else if (ni > 0) { B.status[b] = kNeedsHost; B.lp[b] = NAN; }
             else { B.status[b] = F2M_OK; B.lp[b] = lp; }
         }
-        __syncthreads();
+        T.sync();
     }
 };
 
@@ -958,57 +1122,60 @@ __device__ __forceinline__ Inst make_inst(const Batch& B, int b) {
     I.row = B.row + I.base;
     I.slot = B.slot;
     I.perm = B.perm;
-    I.ef = B.ef + I.row[0];
+    I.gD = B.efD + I.row[0];
+    I.gN = B.efN + I.row[0];
     return I;
 }
 
-// Persistent CTAs take instances from a work counter, largest first.
-template <int T, bool REFIT>
-__global__ void __launch_bounds__(T) k_solve(Batch B, DevParams P, int vcap) {
+// Persistent CTAs; each team takes instances from `items` (largest first).
+template <int TEAM, int TEAMS, bool REFIT>
+__global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, const int32_t* items,
+                                                       int n_items, int32_t* queue, int vcap,
+                                                       int team_bytes) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* FA = reinterpret_cast<double*>(smem_raw);
-    double* FB = FA + vcap;
-    int* efo = reinterpret_cast<int*>(FB + vcap);
-    __shared__ double sred[T / 32];
-    __shared__ long long sredl[T / 32];
-    __shared__ int swarp[T / 32 + 1];
-    __shared__ int s_carry;
-    __shared__ int s_item;
-    Cta<T> C{sred, swarp, &s_carry, sredl};
+    __shared__ double s_red[TEAMS][TEAM / 32];
+    __shared__ long long s_redl[TEAMS][TEAM / 32];
+    __shared__ int s_warp[TEAMS][TEAM / 32 + 1];
+    __shared__ int s_int[TEAMS][4];
+    const int id = threadIdx.x / TEAM;
+    Team<TEAM> T{(int)(threadIdx.x % TEAM), id, s_red[id], s_redl[id], s_warp[id], s_int[id]};
+    unsigned char* mine = smem_raw + (size_t)id * team_bytes;
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(B.queue, 1);
-        __syncthreads();
-        const int item = s_item;
-        __syncthreads();
-        if (item >= B.n_items) return;
-        const int b = B.order[item];
+        if (T.tid == 0) T.sint[0] = atomicAdd(queue, 1);
+        T.sync();
+        const int item = T.sint[0];
+        T.sync();
+        if (item >= n_items) return;
+        const int b = items[item];
         const int st = B.status[b];
         if (REFIT ? (st != F2M_OK && st != kNeedsHost) : (st != F2M_OK)) continue;
         const Inst I = make_inst(B, b);
         if (I.V > vcap) {
-            if (threadIdx.x == 0) B.status[b] = F2M_ERR_CAPACITY;
-            __syncthreads();
+            if (T.tid == 0) B.status[b] = F2M_ERR_CAPACITY;
+            T.sync();
             continue;
         }
-        Solver<T> S(B, P, I, C, FA, FB, efo);
-        double M;
+        const TeamMem M = carve_team(mine, team_bytes, vcap);
+        Solver<TEAM> S(B, P, I, T, M);
+        double Mg;
         if (!REFIT) {
-            for (int v = threadIdx.x; v < I.V; v += T) FA[v] = 0.0;  // graph_cuda_init.hpp:183
-            __syncthreads();
-            M = S.run_start();
+            for (int v = T.tid; v < I.V; v += TEAM) M.Ha[v] = 0.0;  // F = 0, graph_cuda_init.hpp:183
+            T.sync();
+            Mg = S.run_start();
         } else {
             // cuda_IRREGULAR_B_recompute (graph_cuda_comb.hpp:542-574): shift the
             // potentials of irregular combs, 20 frozen iterations, run_fix
-            for (int v = threadIdx.x; v < I.V; v += T) {
-                FA[v] = B.F[I.base + v] + B.shift[I.base + v];
-                efo[v] = B.efcnt[I.base + v];
+            for (int v = T.tid; v < I.V; v += TEAM) {
+                M.Ha[v] = 0.5 * (B.F[I.base + v] + B.shift[I.base + v]);
+                M.efo[v] = B.efcnt[I.base + v];
             }
-            __syncthreads();
-            C.scan_counts(efo, I.V);  // the EF arena still holds the last update_EF
+            T.sync();
+            S.scan_counts();
+            S.load_ef();  // the EF lists of the last update_EF
             for (int go = 0; go < P.frozen_iters; ++go) S.jacobi_masked();
-            M = S.run_fix();
+            Mg = S.run_fix();
         }
-        S.combs_and_primal(b, M, REFIT);
+        S.combs_and_primal(b, Mg, REFIT);
     }
 }
 
@@ -1052,55 +1219,77 @@ cudaError_t launch_graph(const Batch& B, int64_t* deg, int64_t* scan_scratch, cu
     return cudaGetLastError();
 }
 
-size_t solve_smem_bytes(int32_t v_max) {
-    return (size_t)v_max * 2 * sizeof(double) + ((size_t)v_max + 1) * sizeof(int);
-}
-int32_t solve_max_nodes() { return 9000; }
+// Solver classes: instances are routed by point count to a (team width,
+// teams per CTA) shape; every CTA is 1024 threads wide and takes the whole
+// shared memory of an SM, split evenly among its teams.
+struct SolveClass {
+    int team, teams, max_n;
+};
+static const SolveClass kClasses[] = {
+    {128, 8, 448}, {256, 4, 896}, {512, 2, 1792}, {1024, 1, 1 << 30}};
+constexpr int kNumClasses = 4;
 
-template <int T, bool R>
-static int occupancy(size_t smem) {
-    int nb = 0;
-    cudaFuncSetAttribute(k_solve<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_solve<T, R>, T, smem);
-    return nb;
-}
-int solve_blocks_per_sm(int threads, size_t smem) {
-    if (threads == 512) return occupancy<512, false>(smem);
-    if (threads == 128) return occupancy<128, false>(smem);
-    return occupancy<256, false>(smem);
+int32_t solve_max_nodes() { return 10000; }
+int solve_num_classes() { return kNumClasses; }
+int solve_class_of(int32_t n) {
+    for (int c = 0; c < kNumClasses; ++c)
+        if (n <= kClasses[c].max_n) return c;
+    return kNumClasses - 1;
 }
 
-template <bool R>
-static cudaError_t launch_solver(const Batch& B, const DevParams& P, int32_t v_max, int threads,
-                                 cudaStream_t s, int64_t* launches) {
-    if (B.n_items <= 0) return cudaSuccess;
-    const size_t smem = solve_smem_bytes(v_max);
-    int dev = 0, sms = 0;
+static size_t smem_per_block() {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return (size_t)v;
+}
+
+template <int TEAM, int TEAMS, bool R>
+static cudaError_t launch_one(const Batch& B, const DevParams& P, const int32_t* items, int n_items,
+                              int32_t* queue, int vcap, cudaStream_t s, int64_t* launches) {
+    const size_t stat = sizeof(double) * TEAMS * (TEAM / 32) * 2 + sizeof(int) * TEAMS * (TEAM / 32 + 5) + 64;
+    const size_t dyn = (smem_per_block() - stat) & ~(size_t)255;
+    const int team_bytes = (int)((dyn / TEAMS) & ~(size_t)15);
+    if ((size_t)vcap * 20 + 64 > (size_t)team_bytes) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(k_solve<TEAM, TEAMS, R>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int per_sm = 0;
-    if (threads == 512) per_sm = occupancy<512, R>(smem);
-    else if (threads == 128) per_sm = occupancy<128, R>(smem);
-    else per_sm = occupancy<256, R>(smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<TEAM, TEAMS, R>, TEAM * TEAMS, dyn);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int grid = sms * per_sm;
-    if (grid > B.n_items) grid = B.n_items;
-    cudaError_t e = cudaMemsetAsync(B.queue, 0, sizeof(int32_t), s);
-    if (e != cudaSuccess) return e;
-    if (threads == 512) k_solve<512, R><<<grid, 512, smem, s>>>(B, P, v_max);
-    else if (threads == 128) k_solve<128, R><<<grid, 128, smem, s>>>(B, P, v_max);
-    else k_solve<256, R><<<grid, 256, smem, s>>>(B, P, v_max);
+    const int need = (n_items + TEAMS - 1) / TEAMS;
+    if (grid > need) grid = need;
+    if ((e = cudaMemsetAsync(queue, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
+    k_solve<TEAM, TEAMS, R><<<grid, TEAM * TEAMS, dyn, s>>>(B, P, items, n_items, queue, vcap, team_bytes);
     ++*launches;
     return cudaGetLastError();
 }
 
-cudaError_t launch_solve(const Batch& B, const DevParams& P, int32_t v_max, int threads,
-                         cudaStream_t s, int64_t* launches) {
-    return launch_solver<false>(B, P, v_max, threads, s, launches);
+template <bool R>
+static cudaError_t launch_class(int c, const Batch& B, const DevParams& P, const int32_t* items,
+                                int n_items, int32_t* queue, int vcap, cudaStream_t s,
+                                int64_t* launches) {
+    if (n_items <= 0) return cudaSuccess;
+    switch (c) {
+        case 0: return launch_one<128, 8, R>(B, P, items, n_items, queue, vcap, s, launches);
+        case 1: return launch_one<256, 4, R>(B, P, items, n_items, queue, vcap, s, launches);
+        case 2: return launch_one<512, 2, R>(B, P, items, n_items, queue, vcap, s, launches);
+        default: return launch_one<1024, 1, R>(B, P, items, n_items, queue, vcap, s, launches);
+    }
 }
-cudaError_t launch_refit(const Batch& B, const DevParams& P, int32_t v_max, int threads,
-                         cudaStream_t s, int64_t* launches) {
-    return launch_solver<true>(B, P, v_max, threads, s, launches);
+
+cudaError_t launch_solve_class(int c, const Batch& B, const DevParams& P, const int32_t* items,
+                               int n_items, int32_t* queue, int vcap, cudaStream_t s,
+                               int64_t* launches) {
+    return launch_class<false>(c, B, P, items, n_items, queue, vcap, s, launches);
+}
+cudaError_t launch_refit_class(int c, const Batch& B, const DevParams& P, const int32_t* items,
+                               int n_items, int32_t* queue, int vcap, cudaStream_t s,
+                               int64_t* launches) {
+    return launch_class<true>(c, B, P, items, n_items, queue, vcap, s, launches);
 }
 
 }  // namespace f2m

@@ -56,6 +56,8 @@ struct f2m_ctx {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     bool timed = false;
     Batch last{};  // pointers of the last batched call (for the work counters)
+    cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -131,6 +133,9 @@ struct Plan {
     int32_t max_n = 0;
     int32_t N = 0;
     std::vector<int32_t> chunk_inst, chunk_start, order;
+    // order[seg[c] .. seg[c] + cnt[c]) are the instances of solver class c
+    std::vector<int32_t> seg, cnt;
+    std::vector<int32_t> class_vcap;
     int64_t S_cap = 0;
 };
 
@@ -154,6 +159,20 @@ void make_plan(Plan& pl, int32_t n_inst, const int64_t* offs, int32_t N) {
     std::stable_sort(pl.order.begin(), pl.order.end(), [&](int a, int b) {
         return offs[a + 1] - offs[a] > offs[b + 1] - offs[b];
     });
+    // largest first, so the classes are contiguous from the largest down
+    const int nc = solve_num_classes();
+    pl.seg.assign(nc, 0);
+    pl.cnt.assign(nc, 0);
+    pl.class_vcap.assign(nc, 4);
+    for (int32_t b = 0; b < n_inst; ++b) {
+        const int32_t n = (int32_t)(offs[b + 1] - offs[b]);
+        const int c = solve_class_of(n);
+        pl.cnt[c]++;
+        pl.class_vcap[c] = std::max(pl.class_vcap[c], n);
+    }
+    // order holds class nc-1 first (largest instances), then nc-2, ...
+    int32_t acc = 0;
+    for (int c = nc - 1; c >= 0; --c) { pl.seg[c] = acc; acc += pl.cnt[c]; }
     const int64_t Neff = std::min<int64_t>(N, std::max<int32_t>(pl.max_n - 1, 1));
     pl.S_cap = 2 * Neff * std::max<int64_t>(pl.n_total, 1);
 }
@@ -201,7 +220,8 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.slot = A.take<Slot>(S);
     B.perm = A.take<uint16_t>(S);
     B.mirror = A.take<int32_t>(S);
-    B.ef = A.take<Slot>(S);
+    B.efD = A.take<double>(S);
+    B.efN = A.take<uint16_t>(S);
     B.xcode = A.take<uint8_t>(S);
     B.S_cap = S;
     B.F = A.take<double>(n);
@@ -228,15 +248,11 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.n_chunks = (int32_t)pl.chunk_inst.size();
     B.order = *d_order;
     B.n_items = ni;
-    B.queue = A.take<int32_t>(2);
+    B.queue = A.take<int32_t>(8);
     *deg = A.take<int64_t>(n + 1);
     *scan_scratch = A.take<int64_t>(scan_scratch_elems(n) + 1);
 }
 
-int pick_threads(const f2m_params& p, int32_t max_n) {
-    if (p.threads == 128 || p.threads == 256 || p.threads == 512) return p.threads;
-    return max_n > 2048 ? 512 : 256;
-}
 
 /* ------------------------------------------------------------------ */
 /* host comb check and repair loop (the reference's host stage)          */
@@ -527,8 +543,6 @@ struct DevCall {
     int64_t* deg = nullptr;
     int64_t* scan = nullptr;
     int32_t *ci = nullptr, *cs = nullptr, *ord = nullptr;
-    int threads = 256;
-    int32_t vcap = 0;
 };
 
 f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h_offs, int32_t top_k,
@@ -536,15 +550,13 @@ f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h
     make_plan(C.pl, n_inst, h_offs, top_k);
     if (C.pl.max_n > solve_max_nodes())
         return fail(ctx, F2M_ERR_CAPACITY, "instance larger than the CTA solver limit (" +
-                                               std::to_string(solve_max_nodes()) + " points)");
+                                               std::to_string(solve_max_nodes()) + " points per instance)");
     Arena A;
     carve(A, C.B, C.pl, own_inputs, &C.deg, &C.scan, &C.ci, &C.cs, &C.ord);
     F2M_CUDA(ensure_device(ctx, A.used));
     A.base = ctx->dev;
     A.used = 0;
     carve(A, C.B, C.pl, own_inputs, &C.deg, &C.scan, &C.ci, &C.cs, &C.ord);
-    C.threads = pick_threads(prm, C.pl.max_n);
-    C.vcap = std::max<int32_t>(C.pl.max_n, 4);
     // work lists through pinned staging
     const size_t nc = C.pl.chunk_inst.size();
     const size_t bytes = (2 * nc + n_inst) * sizeof(int32_t);
@@ -559,6 +571,24 @@ f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h
     return F2M_OK;
 }
 
+// One persistent launch per solver class, each on its own stream forked from
+// the context stream (largest class first), joined back before returning.
+f2m_status launch_classes(f2m_ctx* ctx, DevCall& C, const f2m_params& prm) {
+    const DevParams P = to_dev(prm);
+    const int nc = solve_num_classes();
+    F2M_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
+    for (int c = nc - 1; c >= 0; --c) {
+        const int n = C.pl.cnt[c];
+        if (n <= 0) continue;
+        F2M_CUDA(cudaStreamWaitEvent(ctx->aux[c], ctx->fork, 0));
+        F2M_CUDA(launch_solve_class(c, C.B, P, C.ord + C.pl.seg[c], n, C.B.queue + c,
+                                    C.pl.class_vcap[c], ctx->aux[c], &ctx->launches));
+        F2M_CUDA(cudaEventRecord(ctx->join[c], ctx->aux[c]));
+        F2M_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[c], 0));
+    }
+    return F2M_OK;
+}
+
 f2m_status run_device(f2m_ctx* ctx, DevCall& C, const f2m_params& prm, bool build_graph, bool solve) {
     F2M_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
     F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
@@ -567,7 +597,10 @@ f2m_status run_device(f2m_ctx* ctx, DevCall& C, const f2m_params& prm, bool buil
     F2M_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
     if (build_graph) F2M_CUDA(launch_graph(C.B, C.deg, C.scan, ctx->stream, &ctx->launches));
     F2M_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
-    if (solve) F2M_CUDA(launch_solve(C.B, to_dev(prm), C.vcap, C.threads, ctx->stream, &ctx->launches));
+    if (solve) {
+        f2m_status s = launch_classes(ctx, C, prm);
+        if (s) return s;
+    }
     F2M_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
     ctx->timed = true;
     ctx->last = C.B;
@@ -652,14 +685,14 @@ f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& 
             steps++;
             HC.shifts(shiftV, type, sh);
             Batch B = C.B;
-            B.n_items = 1;
             const int32_t st = kNeedsHost;
             cudaError_t e;
             if ((e = cudaMemcpyAsync(const_cast<double*>(B.shift) + ibase, sh.data(), sh.size() * sizeof(double),
                                      cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(C.ord, &one, sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(B.status + b, &st, sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
-                (e = launch_refit(B, to_dev(prm), C.vcap, C.threads, ctx->stream, &ctx->launches)) != cudaSuccess ||
+                (e = launch_refit_class(solve_class_of(H.V), B, to_dev(prm), C.ord, 1, B.queue + 7,
+                                        std::max<int32_t>(H.V, 4), ctx->stream, &ctx->launches)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(H.F.data(), B.F + ibase, H.V * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(H.efcnt.data(), B.efcnt + ibase, H.V * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(H.ccnt.data(), B.ccnt + ibase, H.V * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
@@ -809,6 +842,16 @@ f2m_status f2m_create(f2m_ctx** out, int device) {
             delete c;
             return F2M_ERR_CUDA;
         }
+    for (int k = 0; k < 4; ++k)
+        if (cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming) != cudaSuccess) {
+            delete c;
+            return F2M_ERR_CUDA;
+        }
+    if (cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) != cudaSuccess) {
+        delete c;
+        return F2M_ERR_CUDA;
+    }
     *out = c;
     return F2M_OK;
 }
@@ -821,6 +864,11 @@ void f2m_destroy(f2m_ctx* c) {
     if (c->pinned) cudaFreeHost(c->pinned);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
+    for (int k = 0; k < 4; ++k) {
+        if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
+        if (c->join[k]) cudaEventDestroy(c->join[k]);
+    }
+    if (c->fork) cudaEventDestroy(c->fork);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -999,7 +1047,7 @@ f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, cons
     F2M_CUDA(launch_knn(C.B, ctx->stream, &ctx->launches));
     C.B.K_in = nullptr;
     F2M_CUDA(launch_graph(C.B, C.deg, C.scan, ctx->stream, &ctx->launches));
-    F2M_CUDA(launch_solve(C.B, to_dev(prm), C.vcap, C.threads, ctx->stream, &ctx->launches));
+    if ((s = launch_classes(ctx, C, prm))) return s;
     int32_t st = 0;
     F2M_CUDA(cudaMemcpyAsync(&st, C.B.status, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1275,7 +1323,15 @@ f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k, const f
     }
     // graph::RUN (graph_cuda.cu:47-155), timed like dtimeRUN
     auto t0 = std::chrono::steady_clock::now();
-    F2M_CUDA(launch_solve(C.B, to_dev(prm), C.vcap, C.threads, ctx->stream, &ctx->launches));
+    {
+        // the host-assembled graph may have fewer nodes than points: re-plan
+        // the class from the node count
+        std::vector<int32_t> one{0};
+        const int c = solve_class_of(H.V);
+        F2M_CUDA(cudaMemcpyAsync(C.ord, one.data(), sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+        F2M_CUDA(launch_solve_class(c, C.B, to_dev(prm), C.ord, 1, C.B.queue + 6,
+                                    std::max<int32_t>(H.V, 4), ctx->stream, &ctx->launches));
+    }
     F2M_CUDA(cudaMemcpyAsync(&st, C.B.status, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
     if (st != F2M_OK && st != kNeedsHost) return fail(ctx, (f2m_status)st, "the device solve stopped early");
