@@ -53,6 +53,18 @@ struct Batch {
     double* spn;            // size_per_node [n_inst]
     unsigned long long* dmin_bits;  // [n_inst] min edge cost (as ordered bits)
     int32_t* status;        // [n_inst]
+    // cell grid per instance
+    double* gx0;            // [n_inst]
+    double* gy0;
+    double* gh;
+    int32_t* gnx;
+    int32_t* gny;
+    int32_t* pcell;         // [n_total] cell of each point
+    int64_t* cellcnt;       // [n_total+1] points per cell (cells of b at offs[b] + cell)
+    int64_t* cellstart;     // [n_total+1] exclusive scan of cellcnt
+    int32_t* cellcur;       // [n_total]
+    int32_t* sidx;          // [n_total] points sorted by cell (local ids)
+    double2* spt;           // [n_total] their coordinates
     // kNN
     double* cut;            // [n_total]
     int32_t* stat;          // [n_total]
@@ -105,7 +117,7 @@ struct Batch {
 
 // Host-side launchers (f2m_kernels.cu).
 cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches);
-cudaError_t launch_knn(const Batch& B, cudaStream_t s, int64_t* launches);
+cudaError_t launch_knn(const Batch& B, int64_t* scan_scratch, cudaStream_t s, int64_t* launches);
 cudaError_t launch_graph(const Batch& B, int64_t* deg_scratch, int64_t* scan_scratch,
                          cudaStream_t s, int64_t* launches);
 // Persistent solver over items[0..n_items) of size class c (largest first);

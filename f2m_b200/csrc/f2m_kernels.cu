@@ -2,6 +2,7 @@
 //
 // Pipeline of one batched call (one CTA = one instance unless noted):
 //   k_prep      1e-3 rounding, de-duplication, compaction, bbox   (FXY.hpp:231-309)
+//   k_grid_*    per-instance cell grid (counting sort of the points)
 //   k_cutoff    per-node ring cut-off radius (stat pass)          (FXY.hpp:441-534)
 //   k_select    per-node first-N neighbours by (d, emitter, partner)
 //                                                    (FXY.hpp:347-437 + graph_tour.hpp:28-90)
@@ -216,6 +217,23 @@ __global__ void __launch_bounds__(kT) k_prep(Batch B) {
             if (area == 0) st = F2M_ERR_INPUT;
             else spn = sqrt((double)area / (double)V);
         }
+        // cell grid: cells of the ring unit 2*size_per_node, enlarged until
+        // there are at most n cells (they are indexed inside the instance's
+        // point range)
+        double h = 2.0 * spn;
+        if (!(h > 0.0)) h = fmax(fmax(sx, sy), 1.0);
+        long long gx = 1, gy = 1;
+        for (int t = 0; t < 64; ++t) {
+            gx = (long long)(sx / h) + 1;
+            gy = (long long)(sy / h) + 1;
+            if (gx * gy <= (long long)max(n, 1)) break;
+            h *= 1.5;
+        }
+        B.gx0[b] = mnx;
+        B.gy0[b] = mny;
+        B.gh[b] = h;
+        B.gnx[b] = (int)gx;
+        B.gny[b] = (int)gy;
         B.Vn[b] = V;
         B.spn[b] = spn;
         B.status[b] = st;
@@ -224,7 +242,60 @@ __global__ void __launch_bounds__(kT) k_prep(Batch B) {
 }
 
 /* ------------------------------------------------------------------ */
+/* cell grid of each instance (a counting sort of the points by cell)    */
+/* ------------------------------------------------------------------ */
+__device__ __forceinline__ int cell_coord(double v, double v0, double h, int n) {
+    double c = floor((v - v0) / h);
+    c = fmin(fmax(c, 0.0), (double)(n - 1));
+    return (int)c;
+}
+
+__global__ void __launch_bounds__(kT) k_grid_count(Batch B) {
+    const int c = blockIdx.x;
+    const int b = B.chunk_inst[c];
+    if (B.status[b] != F2M_OK) return;
+    const int i = B.chunk_start[c] + threadIdx.x;
+    if (i >= B.Vn[b]) return;
+    const int64_t base = B.offs[b];
+    const double2 p = B.P[base + i];
+    const int nx = B.gnx[b], ny = B.gny[b];
+    const int cell = cell_coord(p.y, B.gy0[b], B.gh[b], ny) * nx + cell_coord(p.x, B.gx0[b], B.gh[b], nx);
+    B.pcell[base + i] = cell;
+    atomicAdd(reinterpret_cast<unsigned long long*>(&B.cellcnt[base + cell]), 1ull);
+}
+
+__global__ void __launch_bounds__(kT) k_grid_scatter(Batch B) {
+    const int c = blockIdx.x;
+    const int b = B.chunk_inst[c];
+    if (B.status[b] != F2M_OK) return;
+    const int i = B.chunk_start[c] + threadIdx.x;
+    if (i >= B.Vn[b]) return;
+    const int64_t base = B.offs[b];
+    const int cell = B.pcell[base + i];
+    const int pos = atomicAdd(&B.cellcur[base + cell], 1);
+    const int64_t k = B.cellstart[base + cell] + pos;
+    B.sidx[k] = i;
+    B.spt[k] = B.P[base + i];
+}
+
+// Cell rows of the box [x-R, x+R] x [y-R, y+R], one cell of margin.
+struct Box {
+    int cx0, cx1, cy0, cy1;
+};
+__device__ __forceinline__ Box box_of(const Batch& B, int b, double x, double y, double R) {
+    const double h = B.gh[b];
+    const int nx = B.gnx[b], ny = B.gny[b];
+    Box r;
+    r.cx0 = max(cell_coord(x - R, B.gx0[b], h, nx) - 1, 0);
+    r.cx1 = min(cell_coord(x + R, B.gx0[b], h, nx) + 1, nx - 1);
+    r.cy0 = max(cell_coord(y - R, B.gy0[b], h, ny) - 1, 0);
+    r.cy1 = min(cell_coord(y + R, B.gy0[b], h, ny) + 1, ny - 1);
+    return r;
+}
+
+/* ------------------------------------------------------------------ */
 /* k_cutoff: ring counting with radius doubling (FXY.hpp:441-534)       */
+/* one warp per node, candidates from the cell grid                     */
 /* ------------------------------------------------------------------ */
 __global__ void __launch_bounds__(kT) k_cutoff(Batch B) {
     const int c = blockIdx.x;
@@ -234,37 +305,35 @@ __global__ void __launch_bounds__(kT) k_cutoff(Batch B) {
     const int i0 = B.chunk_start[c];
     if (i0 >= V) return;
     const int64_t base = B.offs[b];
-    const int i = i0 + threadIdx.x;
-    const bool active = i < V;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int N = min(B.N_cut, V - 1);  // FXY.hpp:77
-    const double s = 2.0 * B.spn[b];  // FXY.hpp:78
-    const double2 me = active ? B.P[base + i] : make_double2(0.0, 0.0);
-    __shared__ double2 tile[kTile];
-
-    int L = 0, st = 0, passes = 0;
-    double cut = 0.0;
-    bool need = active;
-    while (__syncthreads_or(need)) {
-        const double sL = s * (double)L;
-        double lim[5], lo[5], hi[5];
+    const double s = 2.0 * B.spn[b];    // FXY.hpp:78
+    const int nx = B.gnx[b];
+    for (int qi = w; qi < kT && i0 + qi < V; qi += kT / 32) {
+        const int i = i0 + qi;
+        const double2 me = B.P[base + i];
+        int L = 0, st = 0, passes = 0;
+        double cut = 0.0;
+        for (;;) {
+            const double sL = s * (double)L;
+            double lim[5], lo[5], hi[5];
 #pragma unroll
-        for (int j = 0; j < 5; ++j) {
-            lim[j] = fma(s, (double)j, sL);  // nvcc's contraction of s*j + s*L
-            const double l2 = lim[j] * lim[j];
-            lo[j] = l2 * (1.0 - 0x1p-40);
-            hi[j] = l2 * (1.0 + 0x1p-40);
-        }
-        int cnt1 = 0, cnt2 = 0, cnt3 = 0, cnt4 = 0;
-        for (int t0 = 0; t0 < V; t0 += kTile) {
-            const int nt = min(kTile, V - t0);
-            __syncthreads();
-            for (int k = threadIdx.x; k < nt; k += kT) tile[k] = B.P[base + t0 + k];
-            __syncthreads();
-            if (need) {
-                for (int k = 0; k < nt; ++k) {
-                    const double dX = fabs(me.x - tile[k].x), dY = fabs(me.y - tile[k].y);
+            for (int j = 0; j < 5; ++j) {
+                lim[j] = fma(s, (double)j, sL);  // nvcc's contraction of s*j + s*L
+                const double l2 = lim[j] * lim[j];
+                lo[j] = l2 * (1.0 - 0x1p-40);
+                hi[j] = l2 * (1.0 + 0x1p-40);
+            }
+            int cnt1 = 0, cnt2 = 0, cnt3 = 0, cnt4 = 0;
+            const Box bx = box_of(B, b, me.x, me.y, lim[4]);
+            for (int cy = bx.cy0; cy <= bx.cy1; ++cy) {
+                const int64_t k0 = B.cellstart[base + cy * nx + bx.cx0];
+                const int64_t k1 = B.cellstart[base + cy * nx + bx.cx1 + 1];
+                for (int64_t k = k0 + lane; k < k1; k += 32) {
+                    const double2 p = B.spt[k];
+                    const double dX = fabs(me.x - p.x), dY = fabs(me.y - p.y);
                     const double q = fma(dY, dY, dX * dX);
-                    if (q >= hi[4] || t0 + k == i) continue;
+                    if (q >= hi[4] || B.sidx[k] == i) continue;
                     // counts[j] = #{ sqrt(q) < lim[j] } (FXY.hpp:479-482); the
                     // square root is taken only inside the rounding band
                     double d = -1.0;
@@ -282,9 +351,10 @@ __global__ void __launch_bounds__(kT) k_cutoff(Batch B) {
 #undef F2M_RING
                 }
             }
-        }
-        if (need) {
-            const int cnts[5] = {0, cnt1, cnt2, cnt3, cnt4};
+            const int cnts[5] = {0, (int)__reduce_add_sync(0xffffffffu, cnt1),
+                                 (int)__reduce_add_sync(0xffffffffu, cnt2),
+                                 (int)__reduce_add_sync(0xffffffffu, cnt3),
+                                 (int)__reduce_add_sync(0xffffffffu, cnt4)};
             st = 0;
             cut = lim[0];
 #pragma unroll
@@ -293,15 +363,14 @@ __global__ void __launch_bounds__(kT) k_cutoff(Batch B) {
                 cut = lim[j];
                 if (cnts[j] > N) break;
             }
-            if (st >= N) need = false;
-            L = (L == 0) ? 5 : 2 * L;
-            if (++passes >= kMaxPasses) need = false;
+            if (st >= N || ++passes >= kMaxPasses) break;
+            L = (L == 0) ? 5 : 2 * L;  // FXY.hpp:526-531
         }
-    }
-    if (active) {
-        B.cut[base + i] = cut;
-        B.stat[base + i] = st;
-        if (st < N) B.status[b] = F2M_ERR_CAPACITY;
+        if (lane == 0) {
+            B.cut[base + i] = cut;
+            B.stat[base + i] = st;
+            if (st < N) B.status[b] = F2M_ERR_CAPACITY;
+        }
     }
 }
 
@@ -317,7 +386,11 @@ __device__ __forceinline__ bool key_less(double d1, int e1, int o1, double d2, i
     return o1 < o2;
 }
 
-template <int NMAX>
+// One warp per node keeps the sorted first-N list distributed over its
+// lanes (position lane*RPL + r); candidates come from the cells within the
+// node's cut-off radius, which holds all of its first N (their distances are
+// below the cut-off, FXY.hpp:486-502).  Insertion is a warp-wide shift.
+template <int RPL>
 __global__ void __launch_bounds__(kT) k_select(Batch B) {
     const int c = blockIdx.x;
     const int b = B.chunk_inst[c];
@@ -326,54 +399,93 @@ __global__ void __launch_bounds__(kT) k_select(Batch B) {
     const int i0 = B.chunk_start[c];
     if (i0 >= V) return;
     const int64_t base = B.offs[b];
-    const int i = i0 + threadIdx.x;
-    const bool active = i < V;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int N = min(B.N, V - 1);
-    const double2 me = active ? B.P[base + i] : make_double2(0.0, 0.0);
-    __shared__ double2 tile[kTile];
-
-    double kd[NMAX];
-    int ke[NMAX], ko[NMAX];
-    int cnt = 0;
-    double worst_hi = INFINITY;
-    for (int t0 = 0; t0 < V; t0 += kTile) {
-        const int nt = min(kTile, V - t0);
-        __syncthreads();
-        for (int k = threadIdx.x; k < nt; k += kT) tile[k] = B.P[base + t0 + k];
-        __syncthreads();
-        if (!active) continue;
-        for (int k = 0; k < nt; ++k) {
-            const int j = t0 + k;
-            const double dX = fabs(me.x - tile[k].x), dY = fabs(me.y - tile[k].y);
-            const double q = fma(dY, dY, dX * dX);
-            if (q > worst_hi || j == i) continue;
-            const double d = sqrt(q);
-            int em = i, oth = j;
-            if (j < i && d <= B.cut[base + j]) { em = j; oth = i; }
-            int pos;
-            if (cnt == N) {
-                if (!key_less(d, em, oth, kd[N - 1], ke[N - 1], ko[N - 1])) continue;
-                pos = N - 1;
-            } else {
-                pos = cnt++;
+    const int nx = B.gnx[b];
+    const unsigned FULL = 0xffffffffu;
+    for (int qi = w; qi < kT && i0 + qi < V; qi += kT / 32) {
+        const int i = i0 + qi;
+        const double2 me = B.P[base + i];
+        const double R = B.cut[base + i];
+        double kd[RPL];
+        int ke[RPL], ko[RPL];
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) { kd[r] = INFINITY; ke[r] = INT_MAX; ko[r] = INT_MAX; }
+        int cnt = 0;
+        double worst_hi = INFINITY;
+        const Box bx = box_of(B, b, me.x, me.y, R);
+        for (int cy = bx.cy0; cy <= bx.cy1; ++cy) {
+            const int64_t k0 = B.cellstart[base + cy * nx + bx.cx0];
+            const int64_t k1 = B.cellstart[base + cy * nx + bx.cx1 + 1];
+            for (int64_t kb = k0; kb < k1; kb += 32) {
+                const int64_t k = kb + lane;
+                bool pass = false;
+                double d = 0.0;
+                int em = 0, oth = 0;
+                if (k < k1) {
+                    const int j = B.sidx[k];
+                    const double2 p = B.spt[k];
+                    const double dX = fabs(me.x - p.x), dY = fabs(me.y - p.y);
+                    const double q = fma(dY, dY, dX * dX);
+                    if (j != i && (cnt < N || q <= worst_hi)) {
+                        pass = true;
+                        d = sqrt(q);
+                        em = i;
+                        oth = j;
+                        if (j < i && d <= B.cut[base + j]) { em = j; oth = i; }
+                    }
+                }
+                unsigned mask = __ballot_sync(FULL, pass);
+                while (mask) {
+                    const int src = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const double cd = __shfl_sync(FULL, d, src);
+                    const int ce = __shfl_sync(FULL, em, src);
+                    const int co = __shfl_sync(FULL, oth, src);
+                    int mine = 0;
+#pragma unroll
+                    for (int r = 0; r < RPL; ++r)
+                        if (lane * RPL + r < cnt && key_less(kd[r], ke[r], ko[r], cd, ce, co)) mine++;
+                    const int pos = (int)__reduce_add_sync(FULL, mine);
+                    if (pos >= N) continue;
+                    const double pd = __shfl_up_sync(FULL, kd[RPL - 1], 1);
+                    const int pe = __shfl_up_sync(FULL, ke[RPL - 1], 1);
+                    const int po = __shfl_up_sync(FULL, ko[RPL - 1], 1);
+#pragma unroll
+                    for (int r = RPL - 1; r >= 0; --r) {
+                        const int g = lane * RPL + r;
+                        if (g > pos) {
+                            if (r > 0) { kd[r] = kd[r - 1]; ke[r] = ke[r - 1]; ko[r] = ko[r - 1]; }
+                            else { kd[r] = pd; ke[r] = pe; ko[r] = po; }
+                        } else if (g == pos) {
+                            kd[r] = cd; ke[r] = ce; ko[r] = co;
+                        }
+                    }
+                    cnt = min(cnt + 1, N);
+                    if (cnt == N) {
+                        const int wl = (N - 1) / RPL, wr = (N - 1) % RPL;
+                        double mineD = 0.0;
+#pragma unroll
+                        for (int r = 0; r < RPL; ++r)
+                            if (r == wr) mineD = kd[r];
+                        const double wd = __shfl_sync(FULL, mineD, wl);
+                        worst_hi = wd * wd * (1.0 + 0x1p-40);
+                    }
+                }
             }
-            while (pos > 0 && key_less(d, em, oth, kd[pos - 1], ke[pos - 1], ko[pos - 1])) {
-                kd[pos] = kd[pos - 1]; ke[pos] = ke[pos - 1]; ko[pos] = ko[pos - 1];
-                --pos;
-            }
-            kd[pos] = d; ke[pos] = em; ko[pos] = oth;
-            if (cnt == N) worst_hi = kd[N - 1] * kd[N - 1] * (1.0 + 0x1p-40);
         }
-    }
-    if (active) {
         const int64_t o = (base + i) * (int64_t)B.N;
-        B.ntop[base + i] = cnt;
-        for (int k = 0; k < cnt; ++k) {
-            B.top_nbr[o + k] = (ke[k] == i) ? ko[k] : ke[k];
-            B.top_cost[o + k] = kd[k];
-            B.top_em[o + k] = ke[k];
-            B.top_oth[o + k] = ko[k];
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) {
+            const int g = lane * RPL + r;
+            if (g < cnt) {
+                B.top_nbr[o + g] = (ke[r] == i) ? ko[r] : ke[r];
+                B.top_cost[o + g] = kd[r];
+                B.top_em[o + g] = ke[r];
+                B.top_oth[o + g] = ko[r];
+            }
         }
+        if (lane == 0) B.ntop[base + i] = cnt;
     }
 }
 
@@ -1155,7 +1267,7 @@ __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, con
             T.sync();
             continue;
         }
-        const TeamMem M = carve_team(mine, team_bytes, vcap);
+        const TeamMem M = carve_team(mine, team_bytes, I.V);  // sized for this instance
         Solver<TEAM> S(B, P, I, T, M);
         double Mg;
         if (!REFIT) {
@@ -1188,16 +1300,22 @@ cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_knn(const Batch& B, cudaStream_t s, int64_t* launches) {
-    k_cutoff<<<B.n_chunks, kT, 0, s>>>(B);
+cudaError_t launch_knn(const Batch& B, int64_t* scan_scratch, cudaStream_t s, int64_t* launches) {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(B.cellcnt, 0, sizeof(int64_t) * (B.n_total + 1), s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(B.cellcur, 0, sizeof(int32_t) * B.n_total, s)) != cudaSuccess) return e;
+    k_grid_count<<<B.n_chunks, kT, 0, s>>>(B);
     ++*launches;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if (B.N <= 16) k_select<16><<<B.n_chunks, kT, 0, s>>>(B);
-    else if (B.N <= 32) k_select<32><<<B.n_chunks, kT, 0, s>>>(B);
-    else if (B.N <= 64) k_select<64><<<B.n_chunks, kT, 0, s>>>(B);
-    else if (B.N <= 128) k_select<128><<<B.n_chunks, kT, 0, s>>>(B);
-    else k_select<256><<<B.n_chunks, kT, 0, s>>>(B);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_scan(B.cellcnt, B.cellstart, B.n_total, scan_scratch, s, launches)) != cudaSuccess) return e;
+    k_grid_scatter<<<B.n_chunks, kT, 0, s>>>(B);
+    k_cutoff<<<B.n_chunks, kT, 0, s>>>(B);
+    *launches += 2;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (B.N <= 32) k_select<1><<<B.n_chunks, kT, 0, s>>>(B);
+    else if (B.N <= 64) k_select<2><<<B.n_chunks, kT, 0, s>>>(B);
+    else if (B.N <= 128) k_select<4><<<B.n_chunks, kT, 0, s>>>(B);
+    else k_select<8><<<B.n_chunks, kT, 0, s>>>(B);
     ++*launches;
     return cudaGetLastError();
 }

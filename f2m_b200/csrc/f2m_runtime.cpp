@@ -203,6 +203,17 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.spn = A.take<double>(ni);
     B.dmin_bits = A.take<unsigned long long>(ni);
     B.status = A.take<int32_t>(ni);
+    B.gx0 = A.take<double>(ni);
+    B.gy0 = A.take<double>(ni);
+    B.gh = A.take<double>(ni);
+    B.gnx = A.take<int32_t>(ni);
+    B.gny = A.take<int32_t>(ni);
+    B.pcell = A.take<int32_t>(n);
+    B.cellcnt = A.take<int64_t>(n + 1);
+    B.cellstart = A.take<int64_t>(n + 1);
+    B.cellcur = A.take<int32_t>(n);
+    B.sidx = A.take<int32_t>(n);
+    B.spt = A.take<double2>(n);
     B.cut = A.take<double>(n);
     B.stat = A.take<int32_t>(n);
     B.ntop = A.take<int32_t>(n);
@@ -593,7 +604,7 @@ f2m_status run_device(f2m_ctx* ctx, DevCall& C, const f2m_params& prm, bool buil
     F2M_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
     F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
     F2M_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
-    F2M_CUDA(launch_knn(C.B, ctx->stream, &ctx->launches));
+    F2M_CUDA(launch_knn(C.B, C.scan, ctx->stream, &ctx->launches));
     F2M_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
     if (build_graph) F2M_CUDA(launch_graph(C.B, C.deg, C.scan, ctx->stream, &ctx->launches));
     F2M_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
@@ -1044,7 +1055,7 @@ f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, cons
     F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.Y_in), y, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     auto t0 = std::chrono::steady_clock::now();
     F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
-    F2M_CUDA(launch_knn(C.B, ctx->stream, &ctx->launches));
+    F2M_CUDA(launch_knn(C.B, C.scan, ctx->stream, &ctx->launches));
     C.B.K_in = nullptr;
     F2M_CUDA(launch_graph(C.B, C.deg, C.scan, ctx->stream, &ctx->launches));
     if ((s = launch_classes(ctx, C, prm))) return s;
@@ -1267,7 +1278,7 @@ f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k, const f
     F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.X_in), FP.X.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.Y_in), FP.Y.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
-    F2M_CUDA(launch_knn(C.B, ctx->stream, &ctx->launches));
+    F2M_CUDA(launch_knn(C.B, C.scan, ctx->stream, &ctx->launches));
     C.B.K_in = nullptr;
     int32_t st = 0;
     F2M_CUDA(cudaMemcpyAsync(&st, C.B.status, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
