@@ -44,11 +44,20 @@ def parse():
     ap.add_argument("--n-inst", type=int, default=N_INST)
     ap.add_argument("--plain-sample", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size-range", type=int, nargs=2, default=None,
+                    help="keep only instances with lo <= points <= hi (profiling one solver class)")
     return ap.parse_args()
 
 
-def workload(rank, n_inst):
+def workload(rank, n_inst, size_range=None):
     offs, x, y = synth.config3(seed=3 + rank, n_inst=n_inst)
+    if size_range is not None:
+        n = np.diff(offs)
+        keep = np.nonzero((n >= size_range[0]) & (n <= size_range[1]))[0]
+        xs = [x[offs[b]:offs[b + 1]] for b in keep]
+        ys = [y[offs[b]:offs[b + 1]] for b in keep]
+        offs = np.concatenate([[0], np.cumsum(n[keep])]).astype(np.int64)
+        x, y = np.concatenate(xs), np.concatenate(ys)
     return offs, x, y
 
 
@@ -208,7 +217,7 @@ def ours_arm(args, rank, world, local_rank):
     import f2m_b200
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    offs, x, y = workload(rank, args.n_inst)
+    offs, x, y = workload(rank, args.n_inst, args.size_range)
     n_inst = len(offs) - 1
     ctx = f2m_b200.Context(local_rank)
     d_offs = torch.from_numpy(offs).to(dev)

@@ -46,7 +46,7 @@ class Params(ctypes.Structure):
         ("ef_min", ctypes.c_int32), ("comb_thr", ctypes.c_double),
         ("shift0", ctypes.c_double), ("shift_max", ctypes.c_double),
         ("max_iters", ctypes.c_int64), ("cost_mode", ctypes.c_int32),
-        ("threads", ctypes.c_int32),
+        ("solver", ctypes.c_int32),
     ]
 
 

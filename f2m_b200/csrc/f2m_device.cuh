@@ -1,0 +1,197 @@
+// Device helpers shared by the per-team solver (f2m_kernels.cu) and the
+// grid-wide solver (f2m_grid.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "f2m_internal.h"
+
+namespace f2m {
+
+/* ------------------------------------------------------------------ */
+/* block-level helpers                                                  */
+/* ------------------------------------------------------------------ */
+template <int T>
+__device__ __forceinline__ double block_max(double x, double* sred) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    if (lane == 0) sred[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        x = (lane < T / 32) ? sred[lane] : -INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0) sred[0] = x;
+    }
+    __syncthreads();
+    double r = sred[0];
+    __syncthreads();
+    return r;
+}
+template <int T>
+__device__ __forceinline__ double block_min(double x, double* sred) {
+    return -block_max<T>(-x, sred);
+}
+template <int T>
+__device__ __forceinline__ double block_sum(double x, double* sred) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sred[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        x = (lane < T / 32) ? sred[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sred[0] = x;
+    }
+    __syncthreads();
+    double r = sred[0];
+    __syncthreads();
+    return r;
+}
+template <int T>
+__device__ __forceinline__ long long block_sum_ll(long long x, long long* sred) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sred[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        x = (lane < T / 32) ? sred[lane] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sred[0] = x;
+    }
+    __syncthreads();
+    long long r = sred[0];
+    __syncthreads();
+    return r;
+}
+template <int T>
+__device__ __forceinline__ long long block_max_ll(long long x, long long* sred) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = max(x, (long long)__shfl_xor_sync(0xffffffffu, x, o));
+    if (lane == 0) sred[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        x = (lane < T / 32) ? sred[lane] : LLONG_MIN;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = max(x, (long long)__shfl_xor_sync(0xffffffffu, x, o));
+        if (lane == 0) sred[0] = x;
+    }
+    __syncthreads();
+    long long r = sred[0];
+    __syncthreads();
+    return r;
+}
+// Exclusive scan of one int per thread in thread order; *total = block sum.
+// swarp needs T/32 + 1 ints.
+template <int T>
+__device__ __forceinline__ int block_excl_scan(int x, int* swarp, int* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) swarp[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int s = (lane < T / 32) ? swarp[lane] : 0;
+        int incs = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, incs, o);
+            if (lane >= o) incs += y;
+        }
+        if (lane < T / 32) swarp[lane] = incs - s;
+        if (lane == T / 32 - 1) swarp[T / 32] = incs;
+    }
+    __syncthreads();
+    int r = swarp[w] + inc - x;
+    *total = swarp[T / 32];
+    __syncthreads();
+    return r;
+}
+
+struct Inst {
+    int V;
+    int64_t base;          // first node index
+    const int64_t* row;    // row[v], v in [0, V]
+    const Slot* slot;
+    uint16_t* perm;
+    double* gD;            // global EF arena of this instance (D)
+    uint16_t* gN;          // (neighbour)
+};
+
+// The views of instance b inside the batch buffers.
+__device__ __forceinline__ Inst make_inst(const Batch& B, int b) {
+    Inst I;
+    I.V = B.Vn[b];
+    I.base = B.offs[b];
+    I.row = B.row + I.base;
+    I.slot = B.slot;
+    I.perm = B.perm;
+    I.gD = B.efD + I.row[0];
+    I.gN = B.efN + I.row[0];
+    return I;
+}
+
+// Reduced cost of a slot of node v: D + 0.5*F[v1] + 0.5*F[v2] with v1<v2
+// (cuda_recompute_Edges, graph_cuda_grad.hpp:257-268), from H = F/2.
+template <class HP>
+__device__ __forceinline__ double red_d(const Slot& s, int v, HP H, double hv) {
+    const double hn = H[s.nbr];
+    return (v < s.nbr) ? (s.D + hv) + hn : (s.D + hn) + hv;
+}
+
+// Sorted insertion of x into (v0 <= v1 <= v2) keeping the three smallest.
+__device__ __forceinline__ void top3_insert(double x, double& v0, double& v1, double& v2) {
+    const double t = fmax(v0, x);
+    v0 = fmin(v0, x);
+    const double u = fmax(v1, t);
+    v1 = fmin(v1, t);
+    v2 = fmin(v2, u);
+}
+template <class HP>
+__device__ __forceinline__ double pdv(const Inst& I, int64_t r0, const uint16_t* list, int k, int v, HP H,
+                                      double hv) {
+    return red_d(I.slot[r0 + list[k]], v, H, hv);
+}
+
+// qpart_ptr_B (graph_cuda_partition.hpp:3-25), the bound tested first.  On
+// finite values it performs at most size/2 swaps; the pass cap only matters
+// for NaN values (where the reference loops forever) and keeps the kernel
+// finite.
+template <class HP>
+static __device__ int qpart_b(const Inst& I, int64_t r0, int v, HP H, int size, double avg) {
+    uint16_t* list = I.perm + r0;
+    const double hv = H[v];
+    int low = 0, high = size - 1, i = low, j = high;
+    for (int pass = 0; i < j && pass <= size; ++pass) {
+        while (i <= high && pdv(I, r0, list, i, v, H, hv) <= avg) i++;
+        while (j >= low && pdv(I, r0, list, j, v, H, hv) > avg) j--;
+        if (i < j) { const uint16_t t = list[i]; list[i] = list[j]; list[j] = t; }
+    }
+    return j + 1;
+}
+// qpart_ptr_EF (graph_cuda_partition.hpp:27-54): raise the threshold by 1
+// until at least ef_min entries qualify (bounded: see qpart_b).
+template <class HP>
+static __device__ int qpart_ef(const Inst& I, int64_t r0, int v, HP H, int size, double avg,
+                               int ef_min) {
+    if (size < ef_min) return size;  // the reference would not terminate
+    for (int bump = 0; bump < (1 << 20); ++bump) {
+        const int p = qpart_b(I, r0, v, H, size, avg);
+        if (p >= ef_min) return p;
+        avg += 1;
+    }
+    return size;
+}
+
+}  // namespace f2m

@@ -40,6 +40,7 @@ struct Batch {
     int32_t n_inst;
     int32_t N;              // neighbours selected per node (top_k, E_max)
     int32_t N_cut;          // top_k of the cut-off pass (FXY.hpp:77-78); normally N
+    int32_t skip_dedup;     // points were de-duplicated on the host already
     int32_t n_total;        // points over all instances (before de-duplication)
     const int64_t* offs;    // [n_inst+1]
     const double* X_in;     // raw coordinates [n_total]
@@ -115,7 +116,25 @@ struct Batch {
     int32_t* queue;             // persistent-kernel work counter
 };
 
-// Host-side launchers (f2m_kernels.cu).
+// Global state of the grid-wide solver for one large instance (f2m_grid.cu).
+struct GridState {
+    double* Ha;             // [V] H = F/2, two buffers
+    double* Hb;
+    int32_t* efc;           // [V] EF list length of each node
+    double* gD;             // [S] EF lists at their nodes' slot positions (D)
+    uint32_t* gW;           // [S] (neighbour | 1<<31 when it is the lower id)
+    int32_t* scratch;       // [2V] comb prefix lengths + labels
+    int32_t* irr;           // [V]
+    unsigned* bar;          // [2] grid barrier: arrivals, generation
+    int32_t* err;           // [1] set when a barrier timed out
+    double* part;           // [2*grid] partial reductions
+    long long* partl;       // [2*grid]
+};
+constexpr int kGridMaxCtas = 2 * 160;
+
+// Host-side launchers (f2m_kernels.cu, f2m_grid.cu).
+cudaError_t launch_solve_grid(const Batch& B, const DevParams& P, const GridState& G, int b, int V,
+                              bool refit, cudaStream_t s, int64_t* launches);
 cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches);
 cudaError_t launch_knn(const Batch& B, int64_t* scan_scratch, cudaStream_t s, int64_t* launches);
 cudaError_t launch_graph(const Batch& B, int64_t* deg_scratch, int64_t* scan_scratch,

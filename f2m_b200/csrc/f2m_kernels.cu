@@ -21,6 +21,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "f2m_device.cuh"
 #include "f2m_internal.h"
 
 namespace f2m {
@@ -28,116 +29,6 @@ namespace f2m {
 constexpr int kT = 256;       // width of the node-parallel kernels
 constexpr int kTile = 1024;   // points per shared-memory tile (16 KB)
 constexpr int kMaxPasses = 64;
-
-/* ------------------------------------------------------------------ */
-/* block-level helpers                                                  */
-/* ------------------------------------------------------------------ */
-template <int T>
-__device__ __forceinline__ double block_max(double x, double* sred) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
-    if (lane == 0) sred[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        x = (lane < T / 32) ? sred[lane] : -INFINITY;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
-        if (lane == 0) sred[0] = x;
-    }
-    __syncthreads();
-    double r = sred[0];
-    __syncthreads();
-    return r;
-}
-template <int T>
-__device__ __forceinline__ double block_min(double x, double* sred) {
-    return -block_max<T>(-x, sred);
-}
-template <int T>
-__device__ __forceinline__ double block_sum(double x, double* sred) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane == 0) sred[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        x = (lane < T / 32) ? sred[lane] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) sred[0] = x;
-    }
-    __syncthreads();
-    double r = sred[0];
-    __syncthreads();
-    return r;
-}
-template <int T>
-__device__ __forceinline__ long long block_sum_ll(long long x, long long* sred) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane == 0) sred[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        x = (lane < T / 32) ? sred[lane] : 0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) sred[0] = x;
-    }
-    __syncthreads();
-    long long r = sred[0];
-    __syncthreads();
-    return r;
-}
-template <int T>
-__device__ __forceinline__ long long block_max_ll(long long x, long long* sred) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x = max(x, (long long)__shfl_xor_sync(0xffffffffu, x, o));
-    if (lane == 0) sred[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        x = (lane < T / 32) ? sred[lane] : LLONG_MIN;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x = max(x, (long long)__shfl_xor_sync(0xffffffffu, x, o));
-        if (lane == 0) sred[0] = x;
-    }
-    __syncthreads();
-    long long r = sred[0];
-    __syncthreads();
-    return r;
-}
-// Exclusive scan of one int per thread in thread order; *total = block sum.
-// swarp needs T/32 + 1 ints.
-template <int T>
-__device__ __forceinline__ int block_excl_scan(int x, int* swarp, int* total) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int inc = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-    }
-    if (lane == 31) swarp[w] = inc;
-    __syncthreads();
-    if (w == 0) {
-        int s = (lane < T / 32) ? swarp[lane] : 0;
-        int incs = s;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, incs, o);
-            if (lane >= o) incs += y;
-        }
-        if (lane < T / 32) swarp[lane] = incs - s;
-        if (lane == T / 32 - 1) swarp[T / 32] = incs;
-    }
-    __syncthreads();
-    int r = swarp[w] + inc - x;
-    *total = swarp[T / 32];
-    __syncthreads();
-    return r;
-}
 
 __device__ __forceinline__ double round3(double x) {
     double r = round(x * 1000.0);  // std::round: half away from zero, as FXY.hpp:252
@@ -163,7 +54,7 @@ __global__ void __launch_bounds__(kT) k_prep(Batch B) {
     __syncthreads();
     // a point is dropped if an earlier point has identical rounded
     // coordinates; it maps to the first such point (FXY.hpp:260-265)
-    for (int t0 = 0; t0 < n; t0 += kTile) {
+    for (int t0 = 0; t0 < n && !B.skip_dedup; t0 += kTile) {
         const int cnt = min(kTile, n - t0);
         for (int k = threadIdx.x; k < cnt; k += kT) tile[k] = B.Pr[base + t0 + k];
         __syncthreads();
@@ -805,16 +696,6 @@ struct Team {
     }
 };
 
-struct Inst {
-    int V;
-    int64_t base;          // first node index
-    const int64_t* row;    // row[v], v in [0, V]
-    const Slot* slot;
-    uint16_t* perm;
-    double* gD;            // global EF arena of this instance (D)
-    uint16_t* gN;          // (neighbour)
-};
-
 // Shared-memory slice of one team.  H = F/2 is kept instead of F: halving is
 // exact, so H_new = H + grad/2 equals F_new/2 bit for bit and a reduced cost
 // D + 0.5*F[v1] + 0.5*F[v2] is (D + H[v1]) + H[v2] with the same rounding.
@@ -827,12 +708,14 @@ struct TeamMem {
     int cap;
 };
 
+// SINGLE: one H buffer (the Jacobi step keeps its grads in registers).
+template <bool SINGLE>
 __device__ __forceinline__ TeamMem carve_team(unsigned char* base, size_t bytes, int vcap) {
     TeamMem M;
     M.Ha = reinterpret_cast<double*>(base);
-    M.Hb = M.Ha + vcap;
+    M.Hb = SINGLE ? M.Ha : M.Ha + vcap;
     M.efo = reinterpret_cast<int*>(M.Hb + vcap);
-    const size_t used = (size_t)vcap * 16 + (((size_t)vcap + 1) * 4 + 7) / 8 * 8;
+    const size_t used = (size_t)vcap * (SINGLE ? 8 : 16) + (((size_t)vcap + 1) * 4 + 7) / 8 * 8;
     M.eD = reinterpret_cast<double*>(base + used);
     const long long rest = (long long)bytes - (long long)used;
     int cap = rest > 0 ? (int)(rest / 10) : 0;
@@ -846,26 +729,12 @@ __device__ __forceinline__ uint16_t ef_word(int v, int nbr) {
     return (uint16_t)(nbr | (nbr < v ? 0x8000 : 0));
 }
 
-// Reduced cost of a slot of node v: D + 0.5*F[v1] + 0.5*F[v2] with v1<v2
-// (cuda_recompute_Edges, graph_cuda_grad.hpp:257-268), from H = F/2.
-__device__ __forceinline__ double red_d(const Slot& s, int v, const double* H, double hv) {
-    const double hn = H[s.nbr];
-    return (v < s.nbr) ? (s.D + hv) + hn : (s.D + hn) + hv;
-}
-
 // cuda_get_Nodes_grad_R (graph_cuda_grad.hpp:321-340) over a node's EF list:
 // the 2nd and 3rd smallest of {first, rest.., 1e6, 1e6}.  While the first
 // value is below 1e6 the reference's compare chain keeps v0<=v1<=v2 and is a
 // sorted insertion, done here by a branch-free min/max network; otherwise the
 // chain itself runs (it can then leave v0 > v1).  Returns grad/2 = -(v1+v2)/4,
 // the step of H.
-__device__ __forceinline__ void top3_insert(double x, double& v0, double& v1, double& v2) {
-    const double t = fmax(v0, x);
-    v0 = fmin(v0, x);
-    const double u = fmax(v1, t);
-    v1 = fmin(v1, t);
-    v2 = fmin(v2, u);
-}
 __device__ __forceinline__ double ef_half_grad(const double* __restrict__ Dp,
                                                const uint16_t* __restrict__ Wp, int n, double hv,
                                                const double* __restrict__ H) {
@@ -894,41 +763,9 @@ __device__ __forceinline__ double ef_half_grad(const double* __restrict__ Dp,
     return (-(v1 + v2) / 2) * 0.5;
 }
 
-__device__ __forceinline__ double pdv(const Inst& I, int64_t r0, const uint16_t* list, int k, int v,
-                                      const double* H, double hv) {
-    return red_d(I.slot[r0 + list[k]], v, H, hv);
-}
-
-// qpart_ptr_B (graph_cuda_partition.hpp:3-25), the bound tested first.  On
-// finite values it performs at most size/2 swaps; the pass cap only matters
-// for NaN values (where the reference loops forever) and keeps the kernel
-// finite.
-__device__ int qpart_b(const Inst& I, int64_t r0, int v, const double* H, int size, double avg) {
-    uint16_t* list = I.perm + r0;
-    const double hv = H[v];
-    int low = 0, high = size - 1, i = low, j = high;
-    for (int pass = 0; i < j && pass <= size; ++pass) {
-        while (i <= high && pdv(I, r0, list, i, v, H, hv) <= avg) i++;
-        while (j >= low && pdv(I, r0, list, j, v, H, hv) > avg) j--;
-        if (i < j) { const uint16_t t = list[i]; list[i] = list[j]; list[j] = t; }
-    }
-    return j + 1;
-}
-// qpart_ptr_EF (graph_cuda_partition.hpp:27-54): raise the threshold by 1
-// until at least ef_min entries qualify (bounded: see qpart_b).
-__device__ int qpart_ef(const Inst& I, int64_t r0, int v, const double* H, int size, double avg,
-                        int ef_min) {
-    if (size < ef_min) return size;  // the reference would not terminate
-    for (int bump = 0; bump < (1 << 20); ++bump) {
-        const int p = qpart_b(I, r0, v, H, size, avg);
-        if (p >= ef_min) return p;
-        avg += 1;
-    }
-    return size;
-}
-
-template <int TEAM>
+template <int TEAM, bool SINGLE>
 struct Solver {
+    static constexpr int RMAX = 10;  // nodes per thread with one H buffer (V <= 10*TEAM)
     const Batch& B;
     const DevParams& P;
     const Inst& I;
@@ -943,6 +780,9 @@ struct Solver {
 
     __device__ Solver(const Batch& b, const DevParams& p, const Inst& i, const Team<TEAM>& t, TeamMem m)
         : B(b), P(p), I(i), T(t), M(m), Hc(m.Ha), Hn(m.Hb) {}
+    // two ints per node of scratch once the descent is over: the second H
+    // buffer, or the EF area (already spilled to the arena) with one buffer
+    __device__ int* scratch() const { return SINGLE ? reinterpret_cast<int*>(M.eD) : reinterpret_cast<int*>(Hn); }
 
     __device__ int deg(int v) const { return (int)(I.row[v + 1] - I.row[v]); }
     __device__ void swap_f() { double* t = Hc; Hc = Hn; Hn = t; }
@@ -952,25 +792,36 @@ struct Solver {
         const bool sm = o + n <= M.cap;
         return ef_half_grad(sm ? M.eD + o : I.gD + o, sm ? M.eW + o : I.gN + o, n, Hc[v], Hc);
     }
-    // one Jacobi step: F += grad(F) (graph_cuda.cu:293-304), as H += grad/2
-    __device__ void jacobi() {
-        for (int v = T.tid; v < I.V; v += TEAM) Hn[v] = Hc[v] + hgrad(v);
-        wslots += M.efo[I.V];
-        T.sync();
-        swap_f();
-        iters++;
-    }
-    // block_EF_iter_BLOCK (graph_cuda.cu:278-289): frozen nodes keep F
-    __device__ void jacobi_masked() {
-        for (int v = T.tid; v < I.V; v += TEAM) {
-            const double g = hgrad(v);
-            Hn[v] = (B.shift[I.base + v] != 0.0) ? Hc[v] : Hc[v] + g;
+    // one Jacobi step: F += grad(F) (graph_cuda.cu:293-304), as H += grad/2;
+    // frozen nodes keep F (block_EF_iter_BLOCK, graph_cuda.cu:278-289)
+    template <bool MASKED>
+    __device__ __forceinline__ void step() {
+        if (SINGLE) {
+            double g[RMAX];
+#pragma unroll
+            for (int r = 0; r < RMAX; ++r) {
+                const int v = T.tid + r * TEAM;
+                g[r] = (v < I.V) ? hgrad(v) : 0.0;
+            }
+            T.sync();
+#pragma unroll
+            for (int r = 0; r < RMAX; ++r) {
+                const int v = T.tid + r * TEAM;
+                if (v < I.V && !(MASKED && B.shift[I.base + v] != 0.0)) Hc[v] = Hc[v] + g[r];
+            }
+        } else {
+            for (int v = T.tid; v < I.V; v += TEAM) {
+                const double g = hgrad(v);
+                Hn[v] = (MASKED && B.shift[I.base + v] != 0.0) ? Hc[v] : Hc[v] + g;
+            }
         }
         wslots += M.efo[I.V];
         T.sync();
         swap_f();
         iters++;
     }
+    __device__ void jacobi() { step<false>(); }
+    __device__ void jacobi_masked() { step<true>(); }
     // max |grad| (max_node_grad, graph_cuda_maxmin.hpp:29-37)
     __device__ double grad_max() const {
         double m = 0.0;
@@ -1111,7 +962,8 @@ struct Solver {
         const int V = I.V;
         const double porog = P.porog;
         spill_ef();
-        int* ccnt = reinterpret_cast<int*>(Hn);  // Hn is free: room for 2V ints
+        T.sync();  // the EF area may become scratch
+        int* ccnt = scratch();
         int* lab = ccnt + V;
         for (int v = T.tid; v < V; v += TEAM)  // cuda_partition_v3
             ccnt[v] = qpart_b(I, I.row[v], v, Hc, M.efo[v + 1] - M.efo[v], P.comb_thr);
@@ -1227,20 +1079,9 @@ struct Solver {
     }
 };
 
-__device__ __forceinline__ Inst make_inst(const Batch& B, int b) {
-    Inst I;
-    I.V = B.Vn[b];
-    I.base = B.offs[b];
-    I.row = B.row + I.base;
-    I.slot = B.slot;
-    I.perm = B.perm;
-    I.gD = B.efD + I.row[0];
-    I.gN = B.efN + I.row[0];
-    return I;
-}
 
 // Persistent CTAs; each team takes instances from `items` (largest first).
-template <int TEAM, int TEAMS, bool REFIT>
+template <int TEAM, int TEAMS, bool SINGLE, bool REFIT>
 __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, const int32_t* items,
                                                        int n_items, int32_t* queue, int vcap,
                                                        int team_bytes) {
@@ -1267,8 +1108,13 @@ __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, con
             T.sync();
             continue;
         }
-        const TeamMem M = carve_team(mine, team_bytes, I.V);  // sized for this instance
-        Solver<TEAM> S(B, P, I, T, M);
+        if (SINGLE && I.V > Solver<TEAM, SINGLE>::RMAX * TEAM) {
+            if (T.tid == 0) B.status[b] = F2M_ERR_CAPACITY;
+            T.sync();
+            continue;
+        }
+        const TeamMem M = carve_team<SINGLE>(mine, team_bytes, I.V);  // sized for this instance
+        Solver<TEAM, SINGLE> S(B, P, I, T, M);
         double Mg;
         if (!REFIT) {
             for (int v = T.tid; v < I.V; v += TEAM) M.Ha[v] = 0.0;  // F = 0, graph_cuda_init.hpp:183
@@ -1362,26 +1208,26 @@ static size_t smem_per_block() {
     return (size_t)v;
 }
 
-template <int TEAM, int TEAMS, bool R>
+template <int TEAM, int TEAMS, bool SINGLE, bool R>
 static cudaError_t launch_one(const Batch& B, const DevParams& P, const int32_t* items, int n_items,
                               int32_t* queue, int vcap, cudaStream_t s, int64_t* launches) {
     const size_t stat = sizeof(double) * TEAMS * (TEAM / 32) * 2 + sizeof(int) * TEAMS * (TEAM / 32 + 5) + 64;
     const size_t dyn = (smem_per_block() - stat) & ~(size_t)255;
     const int team_bytes = (int)((dyn / TEAMS) & ~(size_t)15);
-    if ((size_t)vcap * 20 + 64 > (size_t)team_bytes) return cudaErrorInvalidConfiguration;
-    cudaError_t e = cudaFuncSetAttribute(k_solve<TEAM, TEAMS, R>,
+    if ((size_t)vcap * (SINGLE ? 20 : 20) + 64 > (size_t)team_bytes) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(k_solve<TEAM, TEAMS, SINGLE, R>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<TEAM, TEAMS, R>, TEAM * TEAMS, dyn);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<TEAM, TEAMS, SINGLE, R>, TEAM * TEAMS, dyn);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int grid = sms * per_sm;
     const int need = (n_items + TEAMS - 1) / TEAMS;
     if (grid > need) grid = need;
     if ((e = cudaMemsetAsync(queue, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
-    k_solve<TEAM, TEAMS, R><<<grid, TEAM * TEAMS, dyn, s>>>(B, P, items, n_items, queue, vcap, team_bytes);
+    k_solve<TEAM, TEAMS, SINGLE, R><<<grid, TEAM * TEAMS, dyn, s>>>(B, P, items, n_items, queue, vcap, team_bytes);
     ++*launches;
     return cudaGetLastError();
 }
@@ -1392,10 +1238,10 @@ static cudaError_t launch_class(int c, const Batch& B, const DevParams& P, const
                                 int64_t* launches) {
     if (n_items <= 0) return cudaSuccess;
     switch (c) {
-        case 0: return launch_one<128, 8, R>(B, P, items, n_items, queue, vcap, s, launches);
-        case 1: return launch_one<256, 4, R>(B, P, items, n_items, queue, vcap, s, launches);
-        case 2: return launch_one<512, 2, R>(B, P, items, n_items, queue, vcap, s, launches);
-        default: return launch_one<1024, 1, R>(B, P, items, n_items, queue, vcap, s, launches);
+        case 0: return launch_one<128, 8, false, R>(B, P, items, n_items, queue, vcap, s, launches);
+        case 1: return launch_one<256, 4, false, R>(B, P, items, n_items, queue, vcap, s, launches);
+        case 2: return launch_one<512, 2, false, R>(B, P, items, n_items, queue, vcap, s, launches);
+        default: return launch_one<1024, 1, false, R>(B, P, items, n_items, queue, vcap, s, launches);
     }
 }
 

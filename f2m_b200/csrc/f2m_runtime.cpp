@@ -126,6 +126,7 @@ DevParams to_dev(const f2m_params& p) {
 /* batch plan + device layout                                           */
 /* ------------------------------------------------------------------ */
 constexpr int kChunk = 256;
+constexpr int32_t kHostDedupPoints = 16384;
 
 struct Plan {
     int32_t n_inst = 0;
@@ -179,6 +180,20 @@ void make_plan(Plan& pl, int32_t n_inst, const int64_t* offs, int32_t N) {
 
 // Carves every buffer of a batched call out of one arena.  With A.base ==
 // nullptr it only measures.
+void carve_grid(Arena& A, GridState& G, int64_t n, int64_t S) {
+    G.Ha = A.take<double>(n);
+    G.Hb = A.take<double>(n);
+    G.efc = A.take<int32_t>(n);
+    G.gD = A.take<double>(S);
+    G.gW = A.take<uint32_t>(S);
+    G.scratch = A.take<int32_t>(2 * n);
+    G.irr = A.take<int32_t>(n);
+    G.bar = A.take<unsigned>(4);
+    G.err = A.take<int32_t>(4);
+    G.part = A.take<double>(2 * kGridMaxCtas);
+    G.partl = A.take<long long>(2 * kGridMaxCtas);
+}
+
 void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, int64_t** scan_scratch,
            int32_t** d_chunk_inst, int32_t** d_chunk_start, int32_t** d_order) {
     const int64_t n = std::max<int64_t>(pl.n_total, 1);
@@ -551,6 +566,8 @@ namespace {
 struct DevCall {
     Plan pl;
     Batch B{};
+    GridState G{};
+    bool grid = false;      // the single large instance runs on the grid-wide solver
     int64_t* deg = nullptr;
     int64_t* scan = nullptr;
     int32_t *ci = nullptr, *cs = nullptr, *ord = nullptr;
@@ -559,15 +576,20 @@ struct DevCall {
 f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h_offs, int32_t top_k,
                       const f2m_params& prm, bool own_inputs) {
     make_plan(C.pl, n_inst, h_offs, top_k);
-    if (C.pl.max_n > solve_max_nodes())
-        return fail(ctx, F2M_ERR_CAPACITY, "instance larger than the CTA solver limit (" +
-                                               std::to_string(solve_max_nodes()) + " points per instance)");
+    C.grid = C.pl.max_n > solve_max_nodes() || (prm.solver == 2 && n_inst == 1);
+    if (C.grid && n_inst > 1)
+        return fail(ctx, F2M_ERR_CAPACITY, "batched instances are limited to " +
+                                               std::to_string(solve_max_nodes()) +
+                                               " points each; solve larger ones one at a time");
     Arena A;
     carve(A, C.B, C.pl, own_inputs, &C.deg, &C.scan, &C.ci, &C.cs, &C.ord);
+    if (C.grid) carve_grid(A, C.G, std::max<int64_t>(C.pl.n_total, 1), C.B.S_cap);
     F2M_CUDA(ensure_device(ctx, A.used));
     A.base = ctx->dev;
     A.used = 0;
     carve(A, C.B, C.pl, own_inputs, &C.deg, &C.scan, &C.ci, &C.cs, &C.ord);
+    if (C.grid) carve_grid(A, C.G, std::max<int64_t>(C.pl.n_total, 1), C.B.S_cap);
+    C.B.skip_dedup = 0;
     // work lists through pinned staging
     const size_t nc = C.pl.chunk_inst.size();
     const size_t bytes = (2 * nc + n_inst) * sizeof(int32_t);
@@ -586,6 +608,10 @@ f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h
 // the context stream (largest class first), joined back before returning.
 f2m_status launch_classes(f2m_ctx* ctx, DevCall& C, const f2m_params& prm) {
     const DevParams P = to_dev(prm);
+    if (C.grid) {
+        F2M_CUDA(launch_solve_grid(C.B, P, C.G, 0, C.pl.max_n, false, ctx->stream, &ctx->launches));
+        return F2M_OK;
+    }
     const int nc = solve_num_classes();
     F2M_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
     for (int c = nc - 1; c >= 0; --c) {
@@ -702,8 +728,9 @@ f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& 
                                      cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(C.ord, &one, sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(B.status + b, &st, sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
-                (e = launch_refit_class(solve_class_of(H.V), B, to_dev(prm), C.ord, 1, B.queue + 7,
-                                        std::max<int32_t>(H.V, 4), ctx->stream, &ctx->launches)) != cudaSuccess ||
+                (e = (C.grid ? launch_solve_grid(B, to_dev(prm), C.G, b, H.V, true, ctx->stream, &ctx->launches)
+                             : launch_refit_class(solve_class_of(H.V), B, to_dev(prm), C.ord, 1, B.queue + 7,
+                                                  std::max<int32_t>(H.V, 4), ctx->stream, &ctx->launches))) != cudaSuccess ||
                 (e = cudaMemcpyAsync(H.F.data(), B.F + ibase, H.V * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(H.efcnt.data(), B.efcnt + ibase, H.V * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(H.ccnt.data(), B.ccnt + ibase, H.V * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
@@ -829,7 +856,7 @@ void f2m_default_params(f2m_params* p) {
     p->shift_max = 32;
     p->max_iters = 20000000;
     p->cost_mode = F2M_COST_REF_EUCLID;
-    p->threads = 0;
+    p->solver = 0;
 }
 
 f2m_status f2m_create(f2m_ctx** out, int device) {
@@ -1041,8 +1068,33 @@ f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, cons
     if (params) prm = *params;
     cudaSetDevice(ctx->device);
     std::unique_ptr<f2m_result> R(new f2m_result());
+    // Large inputs are rounded and de-duplicated on the host, as get_KXY does
+    // (FXY.hpp:252-267); the device's per-instance pass is quadratic.
+    std::vector<double> hx, hy;
+    std::vector<int32_t> hl;
+    bool host_dedup = n > kHostDedupPoints;
+    if (host_dedup) {
+        std::unordered_map<double, std::unordered_map<double, int>> filtr;
+        for (int32_t i = 0; i < n; ++i) {
+            double xx = std::round(x[i] * 1000), yy = std::round(y[i] * 1000);
+            xx /= 1000;
+            yy /= 1000;
+            auto fx = filtr.find(xx);
+            if (fx != filtr.end() && fx->second.count(yy)) continue;
+            filtr[xx][yy] = i;
+            hx.push_back(xx);
+            hy.push_back(yy);
+            hl.push_back(labels ? labels[i] : i + 1);
+        }
+        x = hx.data();
+        y = hy.data();
+        labels = hl.data();
+        n = (int32_t)hx.size();
+    }
+    const int64_t offs2[2] = {0, n};
     DevCall C;
-    if ((s = setup_call(ctx, C, 1, offs, top_k, prm, true))) return s;
+    if ((s = setup_call(ctx, C, 1, offs2, top_k, prm, true))) return s;
+    C.B.skip_dedup = host_dedup ? 1 : 0;
     int32_t* dK = nullptr;
     if (labels) {
         // labels ride in the (unused) cursor buffer until k_prep compacts them
@@ -1050,7 +1102,7 @@ f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, cons
         C.B.K_in = dK;
         F2M_CUDA(cudaMemcpyAsync(dK, labels, n * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
     }
-    F2M_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(C.B.offs), offs, 2 * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(C.B.offs), offs2, 2 * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.X_in), x, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.Y_in), y, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     auto t0 = std::chrono::steady_clock::now();
@@ -1277,6 +1329,7 @@ f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k, const f
     F2M_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(C.B.offs), offs, 2 * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.X_in), FP.X.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.Y_in), FP.Y.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    C.B.skip_dedup = 1;  // parse_tsplib removed the duplicates (FXY.hpp:260-267)
     F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
     F2M_CUDA(launch_knn(C.B, C.scan, ctx->stream, &ctx->launches));
     C.B.K_in = nullptr;
@@ -1334,7 +1387,9 @@ f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k, const f
     }
     // graph::RUN (graph_cuda.cu:47-155), timed like dtimeRUN
     auto t0 = std::chrono::steady_clock::now();
-    {
+    if (C.grid) {
+        F2M_CUDA(launch_solve_grid(C.B, to_dev(prm), C.G, 0, H.V, false, ctx->stream, &ctx->launches));
+    } else {
         // the host-assembled graph may have fewer nodes than points: re-plan
         // the class from the node count
         std::vector<int32_t> one{0};

@@ -57,7 +57,8 @@ typedef struct f2m_params {
     double shift_max;      /* 32 */
     int64_t max_iters;     /* safety cap on Jacobi iterations per solve (not in the reference) */
     int32_t cost_mode;     /* f2m_cost_mode */
-    int32_t threads;       /* CTA width of the batched solver; 0 = autotuned */
+    int32_t solver;        /* 0 auto: a team per instance, the whole GPU above 10,000 points;
+                              2: the whole-GPU solver for a single instance of any size */
 } f2m_params;
 
 typedef struct f2m_ctx f2m_ctx;

@@ -153,3 +153,39 @@ def test_zero_x_span_is_solved(ctx, oracle):
     o = oracle.solve_points(x, y, 6)
     r = ctx.solve_points(x, y, 6)
     _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+
+
+# --- the grid-wide solver (single instances above 10,000 points, or forced) ---
+
+def test_grid_solver_forced_matches_oracle(ctx, oracle):
+    x, y = synth.uniform_int_points(3000, 41)
+    o = oracle.solve_points(x, y, 16)
+    r = ctx.solve_points(x, y, 16, params=f2m_b200.default_params(solver=2))
+    _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+
+
+def test_grid_solver_repair_matches_oracle(ctx, oracle):
+    """The repair loop's device refits on the grid-wide solver."""
+    for seed in (1, 2):
+        x, y = synth.lattice_points(300, seed)
+        o = oracle.solve_points(x, y, 8)
+        r = ctx.solve_points(x, y, 8, params=f2m_b200.default_params(solver=2))
+        _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+        assert r.stats["repair_steps"] == o.stats["repair_steps"] > 0
+
+
+def test_large_instance_uses_grid_solver(ctx, oracle):
+    """20,000 clustered points (the large-instance shape at 1/5 size)."""
+    x, y = synth.config2(2, n=20000)
+    o = oracle.solve_points(x, y, 16, threads=os.cpu_count() or 1)
+    r = ctx.solve_points(x, y, 16)
+    _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+
+
+def test_config2_100k_n50(ctx, oracle):
+    """100,000 points, 64 Gaussian clusters + 10% background, N=50."""
+    x, y = synth.config2(2)
+    o = oracle.solve_points(x, y, 50, threads=os.cpu_count() or 1)
+    r = ctx.solve_points(x, y, 50)
+    _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+    assert abs(r.stats["dual_value"] - r.lp) <= 1e-9 * r.lp
