@@ -1,5 +1,5 @@
 // Internal declarations shared by the CUDA kernels (f2m_kernels.cu) and the
-// host runtime (f2m_runtime.cpp).  Not part of the C ABI.
+// host runtime (f2m_runtime.cu).  Not part of the C ABI.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
