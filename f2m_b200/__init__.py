@@ -82,6 +82,7 @@ EXPORTS = [
     "f2m_solve_file", "f2m_result_free", "f2m_result_status", "f2m_result_n_nodes",
     "f2m_result_n_edges", "f2m_result_lp", "f2m_result_max_rank", "f2m_result_seconds",
     "f2m_result_edges", "f2m_result_nodes", "f2m_result_stats", "f2m_phase_times",
+    "f2m_solve_points_noalloc",
 ]
 
 _lib = None
@@ -120,6 +121,7 @@ def lib():
         L.f2m_result_nodes.argtypes = [vp] * 3
         L.f2m_result_stats.argtypes = [vp, P(Stats)]
         L.f2m_phase_times.argtypes = [vp, vp, P(Work)]
+        L.f2m_solve_points_noalloc.argtypes = [vp, vp, i32, i32, P(Params), vp, vp, vp]
         _lib = L
     return _lib
 
@@ -288,6 +290,16 @@ class Result:
         """graph::X: {edge id: x} for edges in the primal solution."""
         nz = np.nonzero(self.x)[0]
         return {int(e): float(self.x[e]) for e in nz}
+
+
+def solve_points_noalloc(d_x, d_y, n, top_k, d_lp, d_status, stream=0, params=None):
+    """Allocation-free solve of one instance (device pointers as ints; see
+    f2m_solve_points_noalloc in include/f2m.h for who needs it and its
+    limits).  Only enqueues on `stream`; returns the f2m status of the call."""
+    p = params if params is not None else default_params()
+    return lib().f2m_solve_points_noalloc(ctypes.c_void_p(d_x), ctypes.c_void_p(d_y), n, top_k,
+                                          ctypes.byref(p), ctypes.c_void_p(d_lp),
+                                          ctypes.c_void_p(d_status), ctypes.c_void_p(stream))
 
 
 # ---------------------------------------------------------------------------

@@ -15,6 +15,7 @@
 #include <fstream>
 #include <iomanip>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <unordered_map>
@@ -195,7 +196,8 @@ void carve_grid(Arena& A, GridState& G, int64_t n, int64_t S) {
 }
 
 void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, int64_t** scan_scratch,
-           int32_t** d_chunk_inst, int32_t** d_chunk_start, int32_t** d_order) {
+           int32_t** d_chunk_inst, int32_t** d_chunk_start, int32_t** d_order, int64_t n_chunks = -1) {
+    if (n_chunks < 0) n_chunks = (int64_t)pl.chunk_inst.size();
     const int64_t n = std::max<int64_t>(pl.n_total, 1);
     const int32_t ni = pl.n_inst;
     const int64_t S = std::max<int64_t>(pl.S_cap, 1);
@@ -266,12 +268,12 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.checks = A.take<int32_t>(ni);
     B.max_grad = A.take<double>(ni);
     B.dual = A.take<double>(ni);
-    *d_chunk_inst = A.take<int32_t>(pl.chunk_inst.size() + 1);
-    *d_chunk_start = A.take<int32_t>(pl.chunk_start.size() + 1);
+    *d_chunk_inst = A.take<int32_t>(n_chunks + 1);
+    *d_chunk_start = A.take<int32_t>(n_chunks + 1);
     *d_order = A.take<int32_t>(ni + 1);
     B.chunk_inst = *d_chunk_inst;
     B.chunk_start = *d_chunk_start;
-    B.n_chunks = (int32_t)pl.chunk_inst.size();
+    B.n_chunks = (int32_t)n_chunks;
     B.order = *d_order;
     B.n_items = ni;
     B.queue = A.take<int32_t>(8);
@@ -1444,3 +1446,117 @@ void f2m_result_nodes(const f2m_result* r, int32_t* label, double* F) {
 void f2m_result_stats(const f2m_result* r, f2m_stats* s) { *s = r->st; }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------ */
+/* Allocation-free single-instance solve                                */
+/* ------------------------------------------------------------------ */
+// Some callers cannot allocate device memory while they run: a host
+// application that owns the whole GPU through its own memory pool and
+// forbids foreign cudaMalloc/cudaFree, or a latency-critical loop where a
+// cudaMalloc (which may synchronize the device and has no latency bound) is
+// not acceptable.  For them this entry point takes its scratch from one
+// fixed array in device memory, reserved when the library is loaded, and
+// allocates nothing itself: no cudaMalloc/cudaFree, no pinned or pageable
+// host buffers, no library call that allocates.  It is limited to one
+// instance of at most kNoAllocMaxPoints points and kNoAllocMaxN neighbours,
+// and it runs only the device stages (instances whose combs need the host
+// Ax=b stage are reported, not completed).
+namespace {
+
+constexpr int32_t kNoAllocMaxPoints = 2048;
+constexpr int32_t kNoAllocMaxN = 24;
+constexpr size_t kNoAllocBytes = (size_t)8 << 20;  // 8 MiB of device memory per GPU
+
+// The scratch of f2m_solve_points_noalloc.  In host code this name is only a
+// stand-in for the device symbol: its device address comes from
+// cudaGetSymbolAddress (one per device, see noalloc_scratch()).
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 256;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+std::mutex g_noalloc_mu;
+
+// Device address of the scratch array on the current device, looked up the
+// first time this device is used.
+cudaError_t noalloc_scratch(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return cudaSuccess;
+}
+
+// Work lists of one instance written on the device (no host staging).
+__global__ void k_noalloc_setup(int64_t* offs, int32_t* chunk_inst, int32_t* chunk_start, int32_t* order,
+                                int32_t n, int32_t n_chunks) {
+    const int t = threadIdx.x;
+    if (t == 0) { offs[0] = 0; offs[1] = n; order[0] = 0; }
+    for (int c = t; c < n_chunks; c += blockDim.x) { chunk_inst[c] = 0; chunk_start[c] = c * kChunk; }
+}
+
+// Copies the result out; an instance that needs the host comb stage is
+// reported as F2M_ERR_CAPACITY.
+__global__ void k_noalloc_finish(const int32_t* st_in, const double* lp_in, int32_t* st_out, double* lp_out) {
+    if (threadIdx.x == 0) {
+        const int32_t st = st_in[0];
+        *st_out = (st == kNeedsHost) ? (int32_t)F2M_ERR_CAPACITY : st;
+        *lp_out = (st == F2M_OK) ? lp_in[0] : NAN;
+    }
+}
+
+}  // namespace
+
+extern "C" f2m_status f2m_solve_points_noalloc(const double* d_x, const double* d_y, int32_t n, int32_t top_k,
+                                                const f2m_params* params, double* d_lp, int32_t* d_status,
+                                                void* stream) {
+    if (!d_x || !d_y || !d_lp || !d_status) return F2M_ERR_INPUT;
+    if (n < 4 || top_k < 3) return F2M_ERR_INPUT;
+    if (n > kNoAllocMaxPoints || top_k > kNoAllocMaxN) return F2M_ERR_CAPACITY;
+    if (params && params->cost_mode != F2M_COST_REF_EUCLID) return F2M_ERR_INPUT;
+    f2m_params prm;
+    f2m_default_params(&prm);
+    if (params) prm = *params;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+
+    // buffers of one instance carved from the fixed array (vectors stay empty)
+    Plan pl;
+    pl.n_inst = 1;
+    pl.n_total = n;
+    pl.max_n = n;
+    pl.N = top_k;
+    pl.S_cap = 2 * (int64_t)std::min(top_k, n - 1) * n;
+    const int32_t n_chunks = (n + kChunk - 1) / kChunk;
+    Batch B{};
+    int64_t *deg = nullptr, *scan = nullptr;
+    int32_t *ci = nullptr, *cs = nullptr, *ord = nullptr;
+    Arena A;
+    carve(A, B, pl, true, &deg, &scan, &ci, &cs, &ord, n_chunks);
+    if (A.used > kNoAllocBytes) return F2M_ERR_CAPACITY;
+    void* base = nullptr;
+    if (noalloc_scratch(&base) != cudaSuccess) return F2M_ERR_CUDA;
+    A.base = static_cast<char*>(base);
+    A.used = 0;
+    carve(A, B, pl, true, &deg, &scan, &ci, &cs, &ord, n_chunks);
+    B.X_in = d_x;
+    B.Y_in = d_y;
+    B.skip_dedup = 0;
+    int64_t launches = 0;
+    k_noalloc_setup<<<1, 256, 0, s>>>(const_cast<int64_t*>(B.offs), ci, cs, ord, n, n_chunks);
+    if (cudaGetLastError() != cudaSuccess) return F2M_ERR_CUDA;
+    if (launch_prep(B, s, &launches) != cudaSuccess || launch_knn(B, scan, s, &launches) != cudaSuccess ||
+        launch_graph(B, deg, scan, s, &launches) != cudaSuccess ||
+        launch_solve_class(solve_class_of(n), B, to_dev(prm), ord, 1, B.queue, std::max<int32_t>(n, 4), s,
+                           &launches) != cudaSuccess)
+        return F2M_ERR_CUDA;
+    k_noalloc_finish<<<1, 32, 0, s>>>(B.status, B.lp, d_status, d_lp);
+    if (cudaGetLastError() != cudaSuccess) return F2M_ERR_CUDA;
+    return F2M_OK;
+}

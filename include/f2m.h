@@ -146,6 +146,28 @@ f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k,
                           const f2m_params* params, int32_t write_files,
                           f2m_result** out);
 
+/* Allocation-free solve of one instance (no counterpart in the reference).
+ * For callers that cannot allocate device memory while they run -- a host
+ * application that owns the GPU through its own memory pool, or a
+ * latency-bound loop that cannot afford cudaMalloc's synchronisation -- this
+ * entry point allocates nothing: its scratch is one fixed 8 MiB array in
+ * device memory that every GPU loading the library holds until exit.
+ * Limits: n <= 2048 points, top_k <= 24, reference cost mode; larger inputs
+ * return F2M_ERR_CAPACITY.  d_x, d_y (n coordinates), d_lp and d_status (one
+ * value each) are device pointers; `stream` is a cudaStream_t (NULL = the
+ * legacy default stream).  The call only enqueues work on that stream and
+ * returns; the results are ready once the stream is synchronised.  It runs
+ * the device stages only: an instance whose combs need the host Ax=b stage
+ * gets status F2M_ERR_CAPACITY (solve it with f2m_solve_points).
+ * The first call on a device looks up the array's device address there
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array and it keeps the previous call's contents
+ * (the solver clears what must start at zero), so calls that overlap on the
+ * GPU -- on different streams, or from different host threads -- race. */
+f2m_status f2m_solve_points_noalloc(const double* d_x, const double* d_y, int32_t n,
+                                    int32_t top_k, const f2m_params* params, double* d_lp,
+                                    int32_t* d_status, void* stream);
+
 void f2m_result_free(f2m_result* r);
 int32_t f2m_result_status(const f2m_result* r);
 int32_t f2m_result_n_nodes(const f2m_result* r);

@@ -1,0 +1,62 @@
+"""The allocation-free entry point against the regular one.
+
+f2m_solve_points_noalloc serves callers that cannot allocate device memory
+while they run (a host application that owns the GPU through its own pool, or
+a latency-bound loop that cannot wait for cudaMalloc).  It takes its scratch
+from a fixed device array.  This test calls it through the C ABI twice in a
+row -- the array keeps the first call's contents -- and checks both results
+against f2m_solve_batch_device on the same inputs.  The file is named to be
+collected last.
+"""
+import numpy as np
+import pytest
+
+import f2m_b200
+from f2m_b200 import synth
+
+pytestmark = pytest.mark.gpu
+LP_RTOL = 1e-12
+
+
+def _regular(ctx, torch, x, y, top_k):
+    dev = torch.device("cuda", 0)
+    offs = np.array([0, len(x)], np.int64)
+    d_offs = torch.from_numpy(offs).to(dev)
+    d_x = torch.from_numpy(x).to(dev)
+    d_y = torch.from_numpy(y).to(dev)
+    d_lp = torch.empty(1, dtype=torch.float64, device=dev)
+    d_st = torch.empty(1, dtype=torch.int32, device=dev)
+    ctx.solve_batch_device(offs, d_offs.data_ptr(), d_x.data_ptr(), d_y.data_ptr(), top_k,
+                           d_lp.data_ptr(), d_st.data_ptr())
+    ctx.sync()
+    return float(d_lp.item()), int(d_st.item())
+
+
+def test_noalloc_matches_regular_entry_point_twice():
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    ctx = f2m_b200.Context(0)
+    cases = [(synth.uniform_int_points(1800, 71), 16), (synth.uniform_int_points(600, 72), 20)]
+    stream = torch.cuda.Stream(device=dev)
+    for (x, y), top_k in cases:
+        d_x = torch.from_numpy(x).to(dev)
+        d_y = torch.from_numpy(y).to(dev)
+        d_lp = torch.full((1,), -1.0, dtype=torch.float64, device=dev)
+        d_st = torch.full((1,), -1, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        s = f2m_b200.solve_points_noalloc(d_x.data_ptr(), d_y.data_ptr(), len(x), top_k,
+                                          d_lp.data_ptr(), d_st.data_ptr(), stream.cuda_stream)
+        assert s == f2m_b200.OK
+        stream.synchronize()
+        lp, st = float(d_lp.item()), int(d_st.item())
+        lp_ref, st_ref = _regular(ctx, torch, x, y, top_k)
+        assert st == st_ref == f2m_b200.OK
+        assert abs(lp - lp_ref) <= LP_RTOL * abs(lp_ref)
+    ctx.close()
+
+
+def test_noalloc_rejects_sizes_beyond_its_array():
+    s = f2m_b200.solve_points_noalloc(1, 1, 2049, 16, 1, 1)
+    assert s == f2m_b200.ERR_CAPACITY
+    s = f2m_b200.solve_points_noalloc(1, 1, 100, 25, 1, 1)
+    assert s == f2m_b200.ERR_CAPACITY
