@@ -615,10 +615,9 @@ cudaError_t launch_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* scr
 /* ------------------------------------------------------------------ */
 // A CTA holds TEAMS independent teams of TEAM threads.  Each team takes
 // instances from a work counter and keeps, per instance, the potentials F
-// (double-buffered for the Jacobi step), the EF offsets and the EF lists
-// (D as FP64, neighbour as u16) in its slice of shared memory; EF lists that
-// do not fit spill to a global arena at the same offsets.  Team barriers are
-// named barriers (bar.sync id, TEAM).
+// (double-buffered for the Jacobi step) and the EF lists (D as FP64,
+// neighbour as u16) in its slice of shared memory.  Team barriers are named
+// barriers (barrier.sync id, TEAM).
 template <int TEAM>
 struct Team {
     int tid, id;
@@ -626,8 +625,10 @@ struct Team {
     long long* sredl;   // TEAM/32
     int* swarp;         // TEAM/32 + 1
     int* sint;          // 4 ints
+    // barrier.sync without .aligned: a team may reach it with a diverged warp
+    // (after `if (tid == 0) {...}`), which the aligned form (bar.sync) forbids
     __device__ __forceinline__ void sync() const {
-        asm volatile("bar.sync %0, %1;" ::"r"(id + 1), "r"(TEAM) : "memory");
+        asm volatile("barrier.sync %0, %1;" ::"r"(id + 1), "r"(TEAM) : "memory");
     }
     __device__ double max(double x) const {
         const int lane = tid & 31, w = tid >> 5;
@@ -699,73 +700,90 @@ struct Team {
 // Shared-memory slice of one team.  H = F/2 is kept instead of F: halving is
 // exact, so H_new = H + grad/2 equals F_new/2 bit for bit and a reduced cost
 // D + 0.5*F[v1] + 0.5*F[v2] is (D + H[v1]) + H[v2] with the same rounding.
+//
+// The EF lists are stored SELL-32: after each update_EF the nodes are ordered
+// by list length (counting sort, longest first), cut into slices of 32 nodes
+// (one warp), and each slice holds its nodes' entries column-major
+// (entry k of lane l at 32*k + l), padded with +inf to the slice's longest
+// list.  A warp then reads its slice with unit stride and all lanes run the
+// same trip count.  Padding cannot change the three smallest values (it is
+// above the compare chain's 1e6 sentinels).  Slices that do not fit in shared
+// memory are read from the node-indexed copy of the lists in global memory.
 struct TeamMem {
     double* Ha;
     double* Hb;
-    int* efo;        // V+1
-    double* eD;      // cap
-    uint16_t* eW;    // cap: neighbour id | 0x8000 when the neighbour is the lower id
+    int* cnt;        // V+1: EF list length per node (cuda_EF_NodesStat)
+    uint16_t* ord;   // 32*NS: nodes in slice order
+    int* soff;       // NS: slice offset in the SELL arena, -1 = read the global copy
+    int* swid;       // NS: slice width (longest list)
+    int* hist;       // 257: counting-sort buckets
+    double* eD;      // cap entries: D
+    uint16_t* eW;    // cap entries: neighbour | 0x8000 when the neighbour is the lower id
     int cap;
+    int NS;
 };
 
-// SINGLE: one H buffer (the Jacobi step keeps its grads in registers).
-template <bool SINGLE>
-__device__ __forceinline__ TeamMem carve_team(unsigned char* base, size_t bytes, int vcap) {
+__device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+__device__ __forceinline__ TeamMem carve_team(unsigned char* base, size_t bytes, int V) {
     TeamMem M;
-    M.Ha = reinterpret_cast<double*>(base);
-    M.Hb = SINGLE ? M.Ha : M.Ha + vcap;
-    M.efo = reinterpret_cast<int*>(M.Hb + vcap);
-    const size_t used = (size_t)vcap * (SINGLE ? 8 : 16) + (((size_t)vcap + 1) * 4 + 7) / 8 * 8;
-    M.eD = reinterpret_cast<double*>(base + used);
-    const long long rest = (long long)bytes - (long long)used;
+    M.NS = (V + 31) / 32;
+    size_t o = 0;
+    M.Ha = reinterpret_cast<double*>(base + o); o += (size_t)V * 8;
+    M.Hb = reinterpret_cast<double*>(base + o); o += (size_t)V * 8;
+    M.cnt = reinterpret_cast<int*>(base + o); o = align16(o + ((size_t)V + 1) * 4);
+    M.soff = reinterpret_cast<int*>(base + o); o = align16(o + (size_t)M.NS * 4);
+    M.swid = reinterpret_cast<int*>(base + o); o = align16(o + (size_t)M.NS * 4);
+    M.hist = reinterpret_cast<int*>(base + o); o = align16(o + 257 * 4);
+    M.ord = reinterpret_cast<uint16_t*>(base + o); o = align16(o + (size_t)M.NS * 32 * 2);
+    M.eD = reinterpret_cast<double*>(base + o);
+    const long long rest = (long long)bytes - (long long)o;
     int cap = rest > 0 ? (int)(rest / 10) : 0;
-    cap &= ~7;
+    cap &= ~31;
     M.eW = reinterpret_cast<uint16_t*>(M.eD + cap);
     M.cap = cap;
     return M;
+}
+__device__ __host__ inline size_t team_fixed_bytes(int V) {
+    const int NS = (V + 31) / 32;
+    return (size_t)V * 16 + ((size_t)V + 1) * 4 + (size_t)NS * 8 + 257 * 4 + (size_t)NS * 64 + 6 * 16;
 }
 
 __device__ __forceinline__ uint16_t ef_word(int v, int nbr) {
     return (uint16_t)(nbr | (nbr < v ? 0x8000 : 0));
 }
 
-// cuda_get_Nodes_grad_R (graph_cuda_grad.hpp:321-340) over a node's EF list:
-// the 2nd and 3rd smallest of {first, rest.., 1e6, 1e6}.  While the first
-// value is below 1e6 the reference's compare chain keeps v0<=v1<=v2 and is a
-// sorted insertion, done here by a branch-free min/max network; otherwise the
-// chain itself runs (it can then leave v0 > v1).  Returns grad/2 = -(v1+v2)/4,
-// the step of H.
-__device__ __forceinline__ double ef_half_grad(const double* __restrict__ Dp,
-                                               const uint16_t* __restrict__ Wp, int n, double hv,
-                                               const double* __restrict__ H) {
-    auto dv = [&](int k) {
-        const uint16_t w = Wp[k];
-        const double a = H[w & 0x7fff];
-        const bool lo = (w & 0x8000) != 0;
-        return (Dp[k] + (lo ? a : hv)) + (lo ? hv : a);
-    };
-    double v0 = dv(0), v1 = 1e6, v2 = 1e6;
-    if (n >= 3) {
-        const double x1 = dv(1), x2 = dv(2);
-        if (v0 < 1e6) {
-            top3_insert(x1, v0, v1, v2);
-            top3_insert(x2, v0, v1, v2);
-            for (int k = 3; k < n; ++k) top3_insert(dv(k), v0, v1, v2);
-            return (-(v1 + v2) / 2) * 0.5;
+// The reduced cost of an EF entry (D, word) of node v.
+__device__ __forceinline__ double ef_d(double D, uint16_t w, double hv, const double* __restrict__ H) {
+    const double a = H[w & 0x7fff];
+    const bool lo = (w & 0x8000) != 0;
+    return (D + (lo ? a : hv)) + (lo ? hv : a);
+}
+
+// cuda_get_Nodes_grad_R (graph_cuda_grad.hpp:321-340): grad = -(v1+v2)/2 over
+// the 2nd and 3rd smallest of {first, rest.., 1e6, 1e6}.  While the first value
+// is below 1e6 the reference's compare chain keeps v0<=v1<=v2 and is a sorted
+// insertion (top3_insert, a branch-free min/max network); otherwise the chain
+// itself runs (it can then leave v0 > v1).  Returns grad/2, the step of H.
+template <class Get>
+__device__ __forceinline__ double half_grad(int n, Get get) {
+    double v0 = get(0), v1 = 1e6, v2 = 1e6;
+    if (v0 < 1e6) {
+        for (int k = 1; k < n; ++k) top3_insert(get(k), v0, v1, v2);
+    } else {
+        for (int k = 1; k < n; ++k) {
+            const double x = get(k);
+            if (x < v0) { v2 = v1; v1 = v0; v0 = x; continue; }
+            if (x < v1) { v2 = v1; v1 = x; continue; }
+            if (x < v2) { v2 = x; }
         }
-    }
-    for (int k = 1; k < n; ++k) {
-        const double x = dv(k);
-        if (x < v0) { v2 = v1; v1 = v0; v0 = x; continue; }
-        if (x < v1) { v2 = v1; v1 = x; continue; }
-        if (x < v2) { v2 = x; }
     }
     return (-(v1 + v2) / 2) * 0.5;
 }
 
-template <int TEAM, bool SINGLE>
+template <int TEAM>
 struct Solver {
-    static constexpr int RMAX = 10;  // nodes per thread with one H buffer (V <= 10*TEAM)
+    static constexpr int WARPS = TEAM / 32;
     const Batch& B;
     const DevParams& P;
     const Inst& I;
@@ -773,49 +791,46 @@ struct Solver {
     TeamMem M;
     double* Hc;   // H = F/2, current
     double* Hn;   // next (Jacobi double buffer)
+    int64_t row0;
     long long iters = 0;
-    long long wslots = 0;  // active slots read, summed over iterations
+    long long wslots = 0;  // active slots read, summed over iterations (warp leaders)
     int checks = 0;
     bool capped = false;
 
     __device__ Solver(const Batch& b, const DevParams& p, const Inst& i, const Team<TEAM>& t, TeamMem m)
-        : B(b), P(p), I(i), T(t), M(m), Hc(m.Ha), Hn(m.Hb) {}
-    // two ints per node of scratch once the descent is over: the second H
-    // buffer, or the EF area (already spilled to the arena) with one buffer
-    __device__ int* scratch() const { return SINGLE ? reinterpret_cast<int*>(M.eD) : reinterpret_cast<int*>(Hn); }
+        : B(b), P(p), I(i), T(t), M(m), Hc(m.Ha), Hn(m.Hb), row0(i.row[0]) {}
 
     __device__ int deg(int v) const { return (int)(I.row[v + 1] - I.row[v]); }
     __device__ void swap_f() { double* t = Hc; Hc = Hn; Hn = t; }
-    // grad/2 of node v over its EF list
-    __device__ __forceinline__ double hgrad(int v) const {
-        const int o = M.efo[v], n = M.efo[v + 1] - o;
-        const bool sm = o + n <= M.cap;
-        return ef_half_grad(sm ? M.eD + o : I.gD + o, sm ? M.eW + o : I.gN + o, n, Hc[v], Hc);
+
+    // grad/2 of the node in lane `lane` of slice s; v = that node (or -1)
+    __device__ __forceinline__ double slice_hgrad(int s, int lane, int& v) const {
+        const int p = s * 32 + lane;
+        v = (p < I.V) ? (int)M.ord[p] : -1;
+        const int vv = v < 0 ? (int)M.ord[s * 32] : v;  // padding lanes shadow lane 0
+        const double hv = Hc[vv];
+        const int off = M.soff[s];
+        if (off >= 0) {
+            const double* Dp = M.eD + off + lane;
+            const uint16_t* Wp = M.eW + off + lane;
+            return half_grad(M.swid[s], [&](int k) { return ef_d(Dp[32 * k], Wp[32 * k], hv, Hc); });
+        }
+        const int64_t go = I.row[vv] - row0;
+        const double* Dp = I.gD + go;
+        const uint16_t* Wp = I.gN + go;
+        return half_grad(M.cnt[vv], [&](int k) { return ef_d(Dp[k], Wp[k], hv, Hc); });
     }
     // one Jacobi step: F += grad(F) (graph_cuda.cu:293-304), as H += grad/2;
     // frozen nodes keep F (block_EF_iter_BLOCK, graph_cuda.cu:278-289)
     template <bool MASKED>
     __device__ __forceinline__ void step() {
-        if (SINGLE) {
-            double g[RMAX];
-#pragma unroll
-            for (int r = 0; r < RMAX; ++r) {
-                const int v = T.tid + r * TEAM;
-                g[r] = (v < I.V) ? hgrad(v) : 0.0;
-            }
-            T.sync();
-#pragma unroll
-            for (int r = 0; r < RMAX; ++r) {
-                const int v = T.tid + r * TEAM;
-                if (v < I.V && !(MASKED && B.shift[I.base + v] != 0.0)) Hc[v] = Hc[v] + g[r];
-            }
-        } else {
-            for (int v = T.tid; v < I.V; v += TEAM) {
-                const double g = hgrad(v);
-                Hn[v] = (MASKED && B.shift[I.base + v] != 0.0) ? Hc[v] : Hc[v] + g;
-            }
+        const int w = T.tid >> 5, lane = T.tid & 31;
+        for (int s = w; s < M.NS; s += WARPS) {
+            int v;
+            const double g = slice_hgrad(s, lane, v);
+            if (v >= 0) Hn[v] = (MASKED && B.shift[I.base + v] != 0.0) ? Hc[v] : Hc[v] + g;
         }
-        wslots += M.efo[I.V];
+        wslots += M.cnt[I.V];
         T.sync();
         swap_f();
         iters++;
@@ -824,51 +839,94 @@ struct Solver {
     __device__ void jacobi_masked() { step<true>(); }
     // max |grad| (max_node_grad, graph_cuda_maxmin.hpp:29-37)
     __device__ double grad_max() const {
+        const int w = T.tid >> 5, lane = T.tid & 31;
         double m = 0.0;
-        for (int v = T.tid; v < I.V; v += TEAM) m = fmax(m, fabs(hgrad(v)));
+        for (int s = w; s < M.NS; s += WARPS) {
+            int v;
+            const double g = slice_hgrad(s, lane, v);
+            if (v >= 0) m = fmax(m, fabs(g));
+        }
         return 2.0 * T.max(m);
     }
-    // efo[0..V) counts -> exclusive offsets (node order), efo[V] = total
-    __device__ void scan_counts() {
-        int* efo = M.efo;
-        int carry = 0;
-        for (int r = 0; r < I.V; r += TEAM) {
-            const int v = r + T.tid;
-            const int c = (v < I.V) ? efo[v] : 0;
-            int tot;
-            const int ex = T.excl_scan(c, &tot);
-            if (v < I.V) efo[v] = carry + ex;
-            carry += tot;
+    // update_EF (graph_cuda.cu:229-252).  from_perm: copy each node's list
+    // prefix (cnt[v] entries in the order of its permuted list) to the
+    // node-indexed global copy; then build the SELL-32 cache from that copy.
+    __device__ void rebuild_ef(bool from_perm) {
+        const int V = I.V;
+        long long tot = 0;
+        for (int v = T.tid; v < V; v += TEAM) tot += M.cnt[v];
+        if (from_perm) {
+            for (int v = T.tid; v < V; v += TEAM) {
+                const int64_t r0 = I.row[v];
+                const int64_t go = r0 - row0;
+                const int n = M.cnt[v];
+                for (int k = 0; k < n; ++k) {
+                    const Slot s = I.slot[r0 + I.perm[r0 + k]];
+                    I.gD[go + k] = s.D;
+                    I.gN[go + k] = ef_word(v, s.nbr);
+                }
+            }
         }
-        if (T.tid == 0) efo[I.V] = carry;
+        // counting sort by list length, longest first (bucket 255 = 255 or more)
+        for (int k = T.tid; k < 257; k += TEAM) M.hist[k] = 0;
+        tot = T.sum_ll(tot);  // (also orders the hist reset before its use)
+        if (T.tid == 0) M.cnt[V] = (int)tot;
+        for (int v = T.tid; v < V; v += TEAM) atomicAdd(&M.hist[255 - min(M.cnt[v], 255)], 1);
         T.sync();
-    }
-    // update_EF (graph_cuda.cu:229-252): copy each node's list prefix
-    __device__ void rebuild_ef() {
-        for (int v = T.tid; v < I.V; v += TEAM) {
-            const int64_t r0 = I.row[v];
-            const int o = M.efo[v], n = M.efo[v + 1] - o;
-            const bool sm = o + n <= M.cap;
-            double* dD = sm ? M.eD + o : I.gD + o;
-            uint16_t* dW = sm ? M.eW + o : I.gN + o;
-            for (int k = 0; k < n; ++k) {
-                const Slot s = I.slot[r0 + I.perm[r0 + k]];
-                dD[k] = s.D;
-                dW[k] = ef_word(v, s.nbr);
+        if (T.tid == 0) {
+            int run = 0;
+            for (int k = 0; k < 256; ++k) { const int c = M.hist[k]; M.hist[k] = run; run += c; }
+        }
+        T.sync();
+        for (int v = T.tid; v < V; v += TEAM) {
+            const int p = atomicAdd(&M.hist[255 - min(M.cnt[v], 255)], 1);
+            M.ord[p] = (uint16_t)v;
+        }
+        T.sync();
+        // slice widths (longest list of the slice) and offsets in the cache
+        const int w = T.tid >> 5, lane = T.tid & 31;
+        for (int s = w; s < M.NS; s += WARPS) {
+            const int p = s * 32 + lane;
+            const int c = (p < V) ? M.cnt[M.ord[p]] : 0;
+            const int mx = __reduce_max_sync(0xffffffffu, c);
+            if (lane == 0) M.swid[s] = max(mx, 1);
+        }
+        T.sync();
+        int carry = 0;
+        for (int r = 0; r < M.NS; r += TEAM) {
+            const int s = r + T.tid;
+            const int size = (s < M.NS) ? 32 * M.swid[s] : 0;
+            int t;
+            const int ex = T.excl_scan(size, &t);
+            if (s < M.NS) M.soff[s] = (carry + ex + size <= M.cap) ? carry + ex : -1;
+            carry += t;
+        }
+        T.sync();
+        // fill the cached slices from the node-indexed copy
+        for (int s = w; s < M.NS; s += WARPS) {
+            const int off = M.soff[s];
+            if (off < 0) continue;
+            const int p = s * 32 + lane;
+            const int v = (p < V) ? (int)M.ord[p] : -1;
+            const int n = (v >= 0) ? M.cnt[v] : 0;
+            const int64_t go = (v >= 0) ? I.row[v] - row0 : 0;
+            for (int k = 0; k < M.swid[s]; ++k) {
+                const bool real = k < n;
+                M.eD[off + 32 * k + lane] = real ? I.gD[go + k] : INFINITY;
+                M.eW[off + 32 * k + lane] = real ? I.gN[go + k] : (uint16_t)0;
             }
         }
         T.sync();
     }
     __device__ void finish_partition() {
         T.sync();
-        scan_counts();
-        rebuild_ef();
+        rebuild_ef(true);
     }
     // check_OPT + update_EF (graph_cuda.cu:229-271) with cuda_partition_v2
     __device__ double check_opt() {
         for (int v = T.tid; v < I.V; v += TEAM) {
             const int d = deg(v);
-            M.efo[v] = (d < P.ef_small_deg) ? d : qpart_ef(I, I.row[v], v, Hc, d, P.ef_thr, P.ef_min);
+            M.cnt[v] = (d < P.ef_small_deg) ? d : qpart_ef(I, I.row[v], v, Hc, d, P.ef_thr, P.ef_min);
         }
         finish_partition();
         checks++;
@@ -888,19 +946,19 @@ struct Solver {
     }
     // block_GLOB (graph_cuda.cu:363-430)
     __device__ void block_glob() {
-        for (int v = T.tid; v < I.V; v += TEAM) M.efo[v] = min(deg(v), P.glob_K);  // setvalue2V
+        for (int v = T.tid; v < I.V; v += TEAM) M.cnt[v] = min(deg(v), P.glob_K);  // setvalue2V
         finish_partition();
         for (int go = 0; go < P.glob_rounds; ++go) {
             for (int it = 0; it < P.glob_inner; ++it) jacobi();
             // cuda_partition_v4 (graph_cuda_partition.hpp:89-115)
             for (int v = T.tid; v < I.V; v += TEAM) {
                 const int d = deg(v);
-                if (d < P.glob_K) { M.efo[v] = d; continue; }
+                if (d < P.glob_K) { M.cnt[v] = d; continue; }
                 const int64_t r0 = I.row[v];
                 const double hv = Hc[v];
                 double avg = pdv(I, r0, I.perm + r0, 0, v, Hc, hv);
                 for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, I.perm + r0, k, v, Hc, hv));
-                M.efo[v] = qpart_ef(I, r0, v, Hc, d, avg, P.ef_min);
+                M.cnt[v] = qpart_ef(I, r0, v, Hc, d, avg, P.ef_min);
             }
             finish_partition();
             if (grad_max() < P.glob_tol) break;
@@ -931,42 +989,15 @@ struct Solver {
         }
         return M_;
     }
-    // The EF lists in shared memory go to the global arena so that a later
-    // repair step (k_refit) resumes from exactly this update_EF state.
-    // Slots [0, smem_end()) belong to nodes whose whole list is in shared
-    // memory; a node straddling the capacity keeps its list in the arena.
-    __device__ int smem_end() const {
-        long long e = 0;
-        for (int v = T.tid; v <= I.V; v += TEAM)
-            if (M.efo[v] <= M.cap) e = ::max(e, (long long)M.efo[v]);
-        return (int)T.max_ll(e);
-    }
-    __device__ void spill_ef() {
-        const int n = smem_end();
-        for (int k = T.tid; k < n; k += TEAM) {
-            I.gD[k] = M.eD[k];
-            I.gN[k] = M.eW[k];
-        }
-    }
-    __device__ void load_ef() {
-        const int n = smem_end();
-        for (int k = T.tid; k < n; k += TEAM) {
-            M.eD[k] = I.gD[k];
-            M.eW[k] = I.gN[k];
-        }
-        T.sync();
-    }
     // Comb extraction (graph_cuda_comb.hpp:415-475), the device comb check and
     // the primal; writes the per-node state for the host and the results.
     __device__ void combs_and_primal(int b, double M_, bool accumulate) {
         const int V = I.V;
         const double porog = P.porog;
-        spill_ef();
-        T.sync();  // the EF area may become scratch
-        int* ccnt = scratch();
+        int* ccnt = reinterpret_cast<int*>(Hn);  // Hn is free: room for 2V ints
         int* lab = ccnt + V;
         for (int v = T.tid; v < V; v += TEAM)  // cuda_partition_v3
-            ccnt[v] = qpart_b(I, I.row[v], v, Hc, M.efo[v + 1] - M.efo[v], P.comb_thr);
+            ccnt[v] = qpart_b(I, I.row[v], v, Hc, M.cnt[v], P.comb_thr);
         T.sync();
         for (int v = T.tid; v < V; v += TEAM) {
             const int64_t r0 = I.row[v];
@@ -999,16 +1030,16 @@ struct Solver {
             }
             if (T.sum_ll(changed) == 0) break;
         }
-        // state for the host comb check
+        // state for the host comb check (and a later repair step)
         for (int v = T.tid; v < V; v += TEAM) {
             B.F[I.base + v] = 2.0 * Hc[v];
-            B.efcnt[I.base + v] = M.efo[v + 1] - M.efo[v];
+            B.efcnt[I.base + v] = M.cnt[v];
             B.ccnt[I.base + v] = ccnt[v];
         }
         T.sync();
         // comb check (comb::solve_simple, comb_thread.cpp:180-195) with the
         // host's A/B rule (node::get_statusAB, node.cpp:49-57)
-        int* irr = M.efo;  // efo is no longer needed
+        int* irr = M.cnt;  // the EF lengths are saved in B.efcnt
         for (int v = T.tid; v < V; v += TEAM) irr[v] = 0;
         T.sync();
         for (int v = T.tid; v < V; v += TEAM) {
@@ -1079,9 +1110,8 @@ struct Solver {
     }
 };
 
-
 // Persistent CTAs; each team takes instances from `items` (largest first).
-template <int TEAM, int TEAMS, bool SINGLE, bool REFIT>
+template <int TEAM, int TEAMS, bool REFIT>
 __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, const int32_t* items,
                                                        int n_items, int32_t* queue, int vcap,
                                                        int team_bytes) {
@@ -1103,18 +1133,13 @@ __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, con
         const int st = B.status[b];
         if (REFIT ? (st != F2M_OK && st != kNeedsHost) : (st != F2M_OK)) continue;
         const Inst I = make_inst(B, b);
-        if (I.V > vcap) {
+        if (I.V > vcap || team_fixed_bytes(I.V) > (size_t)team_bytes) {
             if (T.tid == 0) B.status[b] = F2M_ERR_CAPACITY;
             T.sync();
             continue;
         }
-        if (SINGLE && I.V > Solver<TEAM, SINGLE>::RMAX * TEAM) {
-            if (T.tid == 0) B.status[b] = F2M_ERR_CAPACITY;
-            T.sync();
-            continue;
-        }
-        const TeamMem M = carve_team<SINGLE>(mine, team_bytes, I.V);  // sized for this instance
-        Solver<TEAM, SINGLE> S(B, P, I, T, M);
+        const TeamMem M = carve_team(mine, team_bytes, I.V);  // sized for this instance
+        Solver<TEAM> S(B, P, I, T, M);
         double Mg;
         if (!REFIT) {
             for (int v = T.tid; v < I.V; v += TEAM) M.Ha[v] = 0.0;  // F = 0, graph_cuda_init.hpp:183
@@ -1122,14 +1147,14 @@ __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, con
             Mg = S.run_start();
         } else {
             // cuda_IRREGULAR_B_recompute (graph_cuda_comb.hpp:542-574): shift the
-            // potentials of irregular combs, 20 frozen iterations, run_fix
+            // potentials of irregular combs, 20 frozen iterations, run_fix; the
+            // EF lists of the last update_EF are in the node-indexed copy
             for (int v = T.tid; v < I.V; v += TEAM) {
                 M.Ha[v] = 0.5 * (B.F[I.base + v] + B.shift[I.base + v]);
-                M.efo[v] = B.efcnt[I.base + v];
+                M.cnt[v] = B.efcnt[I.base + v];
             }
             T.sync();
-            S.scan_counts();
-            S.load_ef();  // the EF lists of the last update_EF
+            S.rebuild_ef(false);
             for (int go = 0; go < P.frozen_iters; ++go) S.jacobi_masked();
             Mg = S.run_fix();
         }
@@ -1208,26 +1233,26 @@ static size_t smem_per_block() {
     return (size_t)v;
 }
 
-template <int TEAM, int TEAMS, bool SINGLE, bool R>
+template <int TEAM, int TEAMS, bool R>
 static cudaError_t launch_one(const Batch& B, const DevParams& P, const int32_t* items, int n_items,
                               int32_t* queue, int vcap, cudaStream_t s, int64_t* launches) {
     const size_t stat = sizeof(double) * TEAMS * (TEAM / 32) * 2 + sizeof(int) * TEAMS * (TEAM / 32 + 5) + 64;
     const size_t dyn = (smem_per_block() - stat) & ~(size_t)255;
     const int team_bytes = (int)((dyn / TEAMS) & ~(size_t)15);
-    if ((size_t)vcap * (SINGLE ? 20 : 20) + 64 > (size_t)team_bytes) return cudaErrorInvalidConfiguration;
-    cudaError_t e = cudaFuncSetAttribute(k_solve<TEAM, TEAMS, SINGLE, R>,
+    if (team_fixed_bytes(vcap) > (size_t)team_bytes) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(k_solve<TEAM, TEAMS, R>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<TEAM, TEAMS, SINGLE, R>, TEAM * TEAMS, dyn);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<TEAM, TEAMS, R>, TEAM * TEAMS, dyn);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int grid = sms * per_sm;
     const int need = (n_items + TEAMS - 1) / TEAMS;
     if (grid > need) grid = need;
     if ((e = cudaMemsetAsync(queue, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
-    k_solve<TEAM, TEAMS, SINGLE, R><<<grid, TEAM * TEAMS, dyn, s>>>(B, P, items, n_items, queue, vcap, team_bytes);
+    k_solve<TEAM, TEAMS, R><<<grid, TEAM * TEAMS, dyn, s>>>(B, P, items, n_items, queue, vcap, team_bytes);
     ++*launches;
     return cudaGetLastError();
 }
@@ -1238,10 +1263,10 @@ static cudaError_t launch_class(int c, const Batch& B, const DevParams& P, const
                                 int64_t* launches) {
     if (n_items <= 0) return cudaSuccess;
     switch (c) {
-        case 0: return launch_one<128, 8, false, R>(B, P, items, n_items, queue, vcap, s, launches);
-        case 1: return launch_one<256, 4, false, R>(B, P, items, n_items, queue, vcap, s, launches);
-        case 2: return launch_one<512, 2, false, R>(B, P, items, n_items, queue, vcap, s, launches);
-        default: return launch_one<1024, 1, false, R>(B, P, items, n_items, queue, vcap, s, launches);
+        case 0: return launch_one<128, 8, R>(B, P, items, n_items, queue, vcap, s, launches);
+        case 1: return launch_one<256, 4, R>(B, P, items, n_items, queue, vcap, s, launches);
+        case 2: return launch_one<512, 2, R>(B, P, items, n_items, queue, vcap, s, launches);
+        default: return launch_one<1024, 1, R>(B, P, items, n_items, queue, vcap, s, launches);
     }
 }
 
