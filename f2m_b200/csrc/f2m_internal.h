@@ -88,6 +88,9 @@ struct Batch {
     double* efD;            // [S] active-set arena (update_EF copies): D
     uint16_t* efN;          // [S] active-set arena: neighbour
     uint8_t* xcode;         // [S] 0, 1 (= 1/2), 2 (= 1)
+    double* selD;           // [S] SELL-32 slices that do not fit in shared memory: D
+    uint16_t* selW;         // [S] ... neighbour word; instance b owns sel_stride * offs[b] ..
+    int64_t sel_stride;     //     sel_stride * offs[b+1] (S / n_total entries per point)
     int64_t S_cap;
     // per-node state kept between the solve and the host comb check
     double* F;              // [n_total] potentials

@@ -707,31 +707,38 @@ struct Team {
 // (entry k of lane l at 32*k + l), padded with +inf to the slice's longest
 // list.  A warp then reads its slice with unit stride and all lanes run the
 // same trip count.  Padding cannot change the three smallest values (it is
-// above the compare chain's 1e6 sentinels).  Slices that do not fit in shared
-// memory are read from the node-indexed copy of the lists in global memory.
+// above the compare chain's 1e6 sentinels).  Slices are cached in shared
+// memory in order; the rest live in the same layout in the instance's part of
+// a global arena (coalesced, L2-resident), and a slice that fits in neither
+// reads each node's list from the node-indexed copy.
 struct TeamMem {
     double* Ha;
     double* Hb;
-    int* cnt;        // V+1: EF list length per node (cuda_EF_NodesStat)
     uint16_t* ord;   // 32*NS: nodes in slice order
-    int* soff;       // NS: slice offset in the SELL arena, -1 = read the global copy
+    int* soff;       // NS: >= 0 shared offset; kSelGlobal + g: global offset g; kSelNode: node copy
     int* swid;       // NS: slice width (longest list)
-    int* hist;       // 257: counting-sort buckets
+    int* hist;       // 257: counting-sort buckets; hist[256] = total list length
     double* eD;      // cap entries: D
     uint16_t* eW;    // cap entries: neighbour | 0x8000 when the neighbour is the lower id
+    double* gsD;     // gcap entries in global memory
+    uint16_t* gsW;
+    int* cnt;        // V: EF list length per node (cuda_EF_NodesStat), global
     int cap;
+    int gcap;
     int NS;
 };
+constexpr int kSelGlobal = -(1 << 30);  // soff in [kSelGlobal, -1]: global SELL
+constexpr int kSelNode = INT_MIN;
 
 __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-__device__ __forceinline__ TeamMem carve_team(unsigned char* base, size_t bytes, int V) {
+__device__ __forceinline__ TeamMem carve_team(unsigned char* base, size_t bytes, const Batch& B, int b,
+                                              int V) {
     TeamMem M;
     M.NS = (V + 31) / 32;
     size_t o = 0;
     M.Ha = reinterpret_cast<double*>(base + o); o += (size_t)V * 8;
-    M.Hb = reinterpret_cast<double*>(base + o); o += (size_t)V * 8;
-    M.cnt = reinterpret_cast<int*>(base + o); o = align16(o + ((size_t)V + 1) * 4);
+    M.Hb = reinterpret_cast<double*>(base + o); o = align16(o + (size_t)V * 8);
     M.soff = reinterpret_cast<int*>(base + o); o = align16(o + (size_t)M.NS * 4);
     M.swid = reinterpret_cast<int*>(base + o); o = align16(o + (size_t)M.NS * 4);
     M.hist = reinterpret_cast<int*>(base + o); o = align16(o + 257 * 4);
@@ -742,11 +749,17 @@ __device__ __forceinline__ TeamMem carve_team(unsigned char* base, size_t bytes,
     cap &= ~31;
     M.eW = reinterpret_cast<uint16_t*>(M.eD + cap);
     M.cap = cap;
+    const int64_t p0 = B.offs[b], p1 = B.offs[b + 1];
+    M.gsD = B.selD + B.sel_stride * p0;
+    M.gsW = B.selW + B.sel_stride * p0;
+    const int64_t gcap = B.sel_stride * (p1 - p0);
+    M.gcap = (int)(gcap < ((int64_t)1 << 29) ? gcap : ((int64_t)1 << 29));
+    M.cnt = B.efcnt + p0;
     return M;
 }
 __device__ __host__ inline size_t team_fixed_bytes(int V) {
     const int NS = (V + 31) / 32;
-    return (size_t)V * 16 + ((size_t)V + 1) * 4 + (size_t)NS * 8 + 257 * 4 + (size_t)NS * 64 + 6 * 16;
+    return (size_t)V * 16 + (size_t)NS * 8 + 257 * 4 + (size_t)NS * 64 + 5 * 16;
 }
 
 __device__ __forceinline__ uint16_t ef_word(int v, int nbr) {
@@ -769,6 +782,7 @@ template <class Get>
 __device__ __forceinline__ double half_grad(int n, Get get) {
     double v0 = get(0), v1 = 1e6, v2 = 1e6;
     if (v0 < 1e6) {
+#pragma unroll 4
         for (int k = 1; k < n; ++k) top3_insert(get(k), v0, v1, v2);
     } else {
         for (int k = 1; k < n; ++k) {
@@ -815,6 +829,11 @@ struct Solver {
             const uint16_t* Wp = M.eW + off + lane;
             return half_grad(M.swid[s], [&](int k) { return ef_d(Dp[32 * k], Wp[32 * k], hv, Hc); });
         }
+        if (off != kSelNode) {
+            const double* Dp = M.gsD + (off - kSelGlobal) + lane;
+            const uint16_t* Wp = M.gsW + (off - kSelGlobal) + lane;
+            return half_grad(M.swid[s], [&](int k) { return ef_d(Dp[32 * k], Wp[32 * k], hv, Hc); });
+        }
         const int64_t go = I.row[vv] - row0;
         const double* Dp = I.gD + go;
         const uint16_t* Wp = I.gN + go;
@@ -830,7 +849,7 @@ struct Solver {
             const double g = slice_hgrad(s, lane, v);
             if (v >= 0) Hn[v] = (MASKED && B.shift[I.base + v] != 0.0) ? Hc[v] : Hc[v] + g;
         }
-        wslots += M.cnt[I.V];
+        wslots += M.hist[256];
         T.sync();
         swap_f();
         iters++;
@@ -870,7 +889,7 @@ struct Solver {
         // counting sort by list length, longest first (bucket 255 = 255 or more)
         for (int k = T.tid; k < 257; k += TEAM) M.hist[k] = 0;
         tot = T.sum_ll(tot);  // (also orders the hist reset before its use)
-        if (T.tid == 0) M.cnt[V] = (int)tot;
+        if (T.tid == 0) M.hist[256] = (int)tot;
         for (int v = T.tid; v < V; v += TEAM) atomicAdd(&M.hist[255 - min(M.cnt[v], 255)], 1);
         T.sync();
         if (T.tid == 0) {
@@ -892,28 +911,43 @@ struct Solver {
             if (lane == 0) M.swid[s] = max(mx, 1);
         }
         T.sync();
+        // slice positions in slice order: the leading slices that fit go to
+        // shared memory, the rest to the global arena (from its start)
         int carry = 0;
+        long long lead = 0;
         for (int r = 0; r < M.NS; r += TEAM) {
             const int s = r + T.tid;
             const int size = (s < M.NS) ? 32 * M.swid[s] : 0;
             int t;
             const int ex = T.excl_scan(size, &t);
-            if (s < M.NS) M.soff[s] = (carry + ex + size <= M.cap) ? carry + ex : -1;
+            if (s < M.NS) {
+                M.soff[s] = carry + ex;
+                if (carry + ex + size <= M.cap) lead = ::max(lead, (long long)(carry + ex + size));
+            }
             carry += t;
         }
+        lead = T.max_ll(lead);
+        for (int s = T.tid; s < M.NS; s += TEAM) {
+            const int pos = M.soff[s], size = 32 * M.swid[s];
+            if (pos + size <= M.cap) continue;
+            const int g = pos - (int)lead;
+            M.soff[s] = (g + size <= M.gcap) ? kSelGlobal + g : kSelNode;
+        }
         T.sync();
-        // fill the cached slices from the node-indexed copy
+        // fill the slices from the node-indexed copy
         for (int s = w; s < M.NS; s += WARPS) {
             const int off = M.soff[s];
-            if (off < 0) continue;
+            if (off == kSelNode) continue;
+            double* dD = (off >= 0) ? M.eD + off : M.gsD + (off - kSelGlobal);
+            uint16_t* dW = (off >= 0) ? M.eW + off : M.gsW + (off - kSelGlobal);
             const int p = s * 32 + lane;
             const int v = (p < V) ? (int)M.ord[p] : -1;
             const int n = (v >= 0) ? M.cnt[v] : 0;
             const int64_t go = (v >= 0) ? I.row[v] - row0 : 0;
             for (int k = 0; k < M.swid[s]; ++k) {
                 const bool real = k < n;
-                M.eD[off + 32 * k + lane] = real ? I.gD[go + k] : INFINITY;
-                M.eW[off + 32 * k + lane] = real ? I.gN[go + k] : (uint16_t)0;
+                dD[32 * k + lane] = real ? I.gD[go + k] : INFINITY;
+                dW[32 * k + lane] = real ? I.gN[go + k] : (uint16_t)0;
             }
         }
         T.sync();
@@ -1030,16 +1064,16 @@ struct Solver {
             }
             if (T.sum_ll(changed) == 0) break;
         }
-        // state for the host comb check (and a later repair step)
+        // state for the host comb check (and a later repair step); the EF
+        // lengths are in B.efcnt already
         for (int v = T.tid; v < V; v += TEAM) {
             B.F[I.base + v] = 2.0 * Hc[v];
-            B.efcnt[I.base + v] = M.cnt[v];
             B.ccnt[I.base + v] = ccnt[v];
         }
         T.sync();
         // comb check (comb::solve_simple, comb_thread.cpp:180-195) with the
         // host's A/B rule (node::get_statusAB, node.cpp:49-57)
-        int* irr = M.cnt;  // the EF lengths are saved in B.efcnt
+        int* irr = ccnt;  // saved in B.ccnt
         for (int v = T.tid; v < V; v += TEAM) irr[v] = 0;
         T.sync();
         for (int v = T.tid; v < V; v += TEAM) {
@@ -1138,7 +1172,7 @@ __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, con
             T.sync();
             continue;
         }
-        const TeamMem M = carve_team(mine, team_bytes, I.V);  // sized for this instance
+        const TeamMem M = carve_team(mine, team_bytes, B, b, I.V);  // sized for this instance
         Solver<TEAM> S(B, P, I, T, M);
         double Mg;
         if (!REFIT) {
@@ -1149,10 +1183,7 @@ __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, con
             // cuda_IRREGULAR_B_recompute (graph_cuda_comb.hpp:542-574): shift the
             // potentials of irregular combs, 20 frozen iterations, run_fix; the
             // EF lists of the last update_EF are in the node-indexed copy
-            for (int v = T.tid; v < I.V; v += TEAM) {
-                M.Ha[v] = 0.5 * (B.F[I.base + v] + B.shift[I.base + v]);
-                M.cnt[v] = B.efcnt[I.base + v];
-            }
+            for (int v = T.tid; v < I.V; v += TEAM) M.Ha[v] = 0.5 * (B.F[I.base + v] + B.shift[I.base + v]);
             T.sync();
             S.rebuild_ef(false);
             for (int go = 0; go < P.frozen_iters; ++go) S.jacobi_masked();

@@ -251,6 +251,9 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.efD = A.take<double>(S);
     B.efN = A.take<uint16_t>(S);
     B.xcode = A.take<uint8_t>(S);
+    B.selD = A.take<double>(S);
+    B.selW = A.take<uint16_t>(S);
+    B.sel_stride = S / n;
     B.S_cap = S;
     B.F = A.take<double>(n);
     B.efcnt = A.take<int32_t>(n);
