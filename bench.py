@@ -8,6 +8,7 @@ A step is one full solve of the whole batch: rounding and de-duplication, kNN
 graph, dual descent, comb extraction and the primal value of every instance.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --workload large      # one 100,000-point clustered instance, N = 50
 
 Under torchrun each rank solves its own 4,096-instance batch (seed 3 + rank);
 the job time is the max over ranks.  `--impl reference` times the CPU
@@ -41,6 +42,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "large"],
+                    help="batch: 4,096 mixed-size instances (the headline); large: one "
+                         "100,000-point Gaussian-mixture instance with N=50 (grid-wide solver)")
+    ap.add_argument("--large-n", type=int, default=100_000, help="points of the large instance")
     ap.add_argument("--n-inst", type=int, default=N_INST)
     ap.add_argument("--plain-sample", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -164,6 +169,13 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def alg_bytes(work):
+    """Algorithmic bytes of the dual iterations: per swept (active) slot the
+    12-byte (D, neighbour) record, per node 28 bytes (F in, F out, list offset,
+    gathered F counted once per node)."""
+    return 12.0 * work["slot_iters"] + 28.0 * work["node_iters"]
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -172,11 +184,17 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the solver kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_solve_traffic.json")
-    if os.path.exists(p):
-        return json.load(open(p))
+def profile_traffic(workload, work):
+    """DRAM bytes of the solve phase, scaled from the committed ncu summary of a
+    smaller case by the dual-iteration work (node iterations), or None.  The
+    summary holds a line `traffic_per_node_iter <workload> <bytes>`."""
+    p = os.path.join(ROOT, "profiles", "k_solve_dram_traffic.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) == 3 and f[0] == "traffic_per_node_iter" and f[1] == workload:
+            return float(f[2]) * work["node_iters"]
     return None
 
 
@@ -312,13 +330,10 @@ def ours_arm(args, rank, world, local_rank):
         return
     # roofline of the dominant kernel: the persistent solver
     peak, peak_kind = measured_peak()
-    # algorithmic bytes of a Jacobi iteration: per active slot the 12-byte
-    # (D, nbr) record and the gathered 8-byte F; per node F read + write and
-    # the two EF offsets (24 bytes)
-    alg_bytes = 20.0 * work["slot_iters"] + 24.0 * work["node_iters"]
+    ab = alg_bytes(work)
     solve_ms = phase[3]
-    achieved = alg_bytes / (solve_ms / 1e3) / 1e9
-    tr = profile_traffic()
+    achieved = ab / (solve_ms / 1e3) / 1e9
+    tr = profile_traffic("batch", work)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_job,
@@ -327,8 +342,8 @@ def ours_arm(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "kernel": "k_solve (persistent CTA-per-instance solver)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": (tr["dram_bytes_per_launch_scaled"] if tr else None),
-                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "traffic": tr,
+                     "algorithmic_bytes_per_launch": ab,
                      "note": "active set and potentials stay in SMEM/L1 across iterations; "
                              "frac > 1 reflects on-chip reuse, traffic is the DRAM bytes"},
         "e2e": {"value": n_inst * world / (e2e / 1e3), "unit": "solves/s",
@@ -337,7 +352,8 @@ def ours_arm(args, rank, world, local_rank):
         "clocks": clocks,
         "gpu_launches": int(launches // max(args.steps, 1)),
         "gpu_launches_total": int(launches),
-        "phases_ms": {"prep": phase[0], "knn": phase[1], "graph": phase[2], "solve": phase[3]},
+        "phases_ms": {"prep": phase[0], "knn": phase[1], "graph": phase[2], "solve": phase[3],
+                      "host_and_copies": ms - float(np.sum(phase))},
         "work": work,
         "plain_loop": {"value": plain, "unit": "solves/s", "sample": f"{len(sample)} instances, "
                        "one f2m_solve_batch_device call each", "speedup": value / world / plain,
@@ -346,6 +362,71 @@ def ours_arm(args, rank, world, local_rank):
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(offs, x, y)
+    print(json.dumps(line), flush=True)
+
+
+def large_arm(args, rank, world, local_rank):
+    """One 100,000-point instance (64 Gaussian clusters + 10% background), N=50:
+    replicas only (the instance does not shard); the grid-wide solver."""
+    import torch
+
+    import f2m_b200
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    x, y = synth.config2(2 + rank, n=args.large_n)
+    n_large = 50
+    ctx = f2m_b200.Context(local_rank)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        r = ctx.solve_points(x, y, n_large)
+    assert r.status == 0
+    clk = Clocks(local_rank)
+    l0 = ctx.kernel_launches()
+    wall, phase = [], np.zeros(4)
+    clk.start()
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = ctx.solve_points(x, y, n_large)
+        wall.append(1e3 * (time.perf_counter() - t0))
+        ph, work = ctx.phase_times()
+        phase += ph
+    clocks = clk.stop()
+    launches = ctx.kernel_launches() - l0
+    phase /= args.steps
+    dev_ms = float(np.sum(phase))
+    e2e_ms = float(np.mean(wall))
+    t = [dev_ms, e2e_ms]
+    if world > 1:
+        tt = torch.tensor(t, dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t = tt.tolist()
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peak()
+    ab = alg_bytes(work)
+    achieved = ab / (phase[3] / 1e3) / 1e9
+    line = {
+        "metric": "F2M solves/s, one large clustered instance", "value": world * 1e3 / t[0],
+        "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t[0], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.large_n:,} points: 64 Gaussian clusters (sigma 0.5% of a "
+                               "10^6 box) + 10% uniform background, rounded; N=50", "top_k": n_large,
+                   "seed": "2 + rank", "parallelism": f"replicas on {world} GPU(s)",
+                   "l2": f"flushed between timed steps ({FLUSH_BYTES >> 20} MiB write)"},
+        "roofline": {"bound": "hbm", "kernel": "k_solve_grid (grid-wide dual descent)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": profile_traffic("large", work),
+                     "algorithmic_bytes_per_launch": ab},
+        "e2e": {"value": world * 1e3 / t[1], "unit": "solves/s",
+                "h2d_bytes_per_step": int(x.nbytes + y.nbytes), "d2h_bytes_per_step": None},
+        "clocks": clocks, "gpu_launches": int(launches // max(args.steps, 1)),
+        "phases_ms": {"prep": phase[0], "knn": phase[1], "graph": phase[2], "solve": phase[3]},
+        "work": work, "lp": r.lp, "n_nodes": r.n_nodes, "n_edges": r.n_edges,
+        "iterations": int(r.stats["iterations"]) if "iterations" in r.stats else None,
+    }
     print(json.dumps(line), flush=True)
 
 
@@ -366,6 +447,8 @@ def main():
     try:
         if args.impl == "reference":
             reference_arm(args, rank, world)
+        elif args.workload == "large":
+            large_arm(args, rank, world, local_rank)
         else:
             ours_arm(args, rank, world, local_rank)
     finally:

@@ -182,14 +182,38 @@ static __device__ int qpart_b(const Inst& I, int64_t r0, int v, HP H, int size, 
 }
 // qpart_ptr_EF (graph_cuda_partition.hpp:27-54): raise the threshold by 1
 // until at least ef_min entries qualify (bounded: see qpart_b).
+//
+// A pass whose threshold t stays below the smallest value g of the upper part
+// left by the previous pass finds the list already partitioned for t: the
+// i-scan stops at the first upper entry, the j-scan at the last lower one, no
+// swap happens and the count repeats.  Such passes are counted but not run,
+// so the threshold sequence (repeated FP64 `avg += 1`), the final order and
+// the count are those of the plain loop.  With a NaN in the list every pass
+// runs.
 template <class HP>
 static __device__ int qpart_ef(const Inst& I, int64_t r0, int v, HP H, int size, double avg,
                                int ef_min) {
     if (size < ef_min) return size;  // the reference would not terminate
-    for (int bump = 0; bump < (1 << 20); ++bump) {
+    constexpr int kLimit = 1 << 20;
+    const uint16_t* list = I.perm + r0;
+    const double hv = H[v];
+    for (int bump = 0; bump < kLimit;) {
         const int p = qpart_b(I, r0, v, H, size, avg);
         if (p >= ef_min) return p;
+        double g = INFINITY;
+        bool nan = false;
+        for (int k = 0; k < size; ++k) {
+            const double d = pdv(I, r0, list, k, v, H, hv);
+            nan |= (d != d);
+            if (k >= p) g = fmin(g, d);
+        }
         avg += 1;
+        ++bump;
+        if (nan) continue;
+        while (avg < g && bump < kLimit) {
+            avg += 1;
+            ++bump;
+        }
     }
     return size;
 }

@@ -38,6 +38,7 @@ struct GridSolver {
     double* sred;
     long long* sredl;
     int* swarp;
+    unsigned long long* sbcv;  // shared broadcast slot of the grid reductions
     int phase = 0;
     long long iters = 0, wslots = 0;
     int checks = 0;
@@ -72,46 +73,44 @@ struct GridSolver {
         dead = *(volatile int*)G.err != 0;
         return !dead;
     }
-    // deterministic grid reductions through per-CTA partials (double-buffered)
-    __device__ double gmax(double x) {
-        x = block_max<kGT>(x, sred);
-        if (threadIdx.x == 0) G.part[phase * gridDim.x + blockIdx.x] = x;
+    // Deterministic grid reductions through per-CTA partials (double-buffered).
+    // After the barrier one warp per CTA reads the partials (lane-strided, then
+    // a fixed shuffle tree) and broadcasts through shared memory, so every CTA
+    // computes the same value in the same order.
+    template <class T, class Op>
+    __device__ T greduce(T x, T* part, T ident, Op op) {
+        if (threadIdx.x == 0) part[phase * gridDim.x + blockIdx.x] = x;
         sync();
-        double r = -INFINITY;
-        const volatile double* pp = G.part + phase * gridDim.x;
-        for (unsigned k = 0; k < gridDim.x; ++k) r = fmax(r, pp[k]);
+        if (threadIdx.x < 32) {
+            const volatile T* pp = part + phase * gridDim.x;
+            T r = ident;
+            for (unsigned k = threadIdx.x; k < gridDim.x; k += 32) r = op(r, pp[k]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) r = op(r, __shfl_xor_sync(0xffffffffu, r, o));
+            if (threadIdx.x == 0) *reinterpret_cast<T*>(sbcv) = r;
+        }
+        __syncthreads();
+        const T r = *reinterpret_cast<const T*>(sbcv);
+        __syncthreads();
         phase ^= 1;
         return r;
+    }
+    __device__ double gmax(double x) {
+        x = block_max<kGT>(x, sred);
+        return greduce<double>(x, G.part, -INFINITY, [](double a, double b) { return fmax(a, b); });
     }
     __device__ double gsum(double x) {
         x = block_sum<kGT>(x, sred);
-        if (threadIdx.x == 0) G.part[phase * gridDim.x + blockIdx.x] = x;
-        sync();
-        double r = 0.0;
-        const volatile double* pp = G.part + phase * gridDim.x;
-        for (unsigned k = 0; k < gridDim.x; ++k) r += pp[k];
-        phase ^= 1;
-        return r;
+        return greduce<double>(x, G.part, 0.0, [](double a, double b) { return a + b; });
     }
     __device__ long long gsum_ll(long long x) {
         x = block_sum_ll<kGT>(x, sredl);
-        if (threadIdx.x == 0) G.partl[phase * gridDim.x + blockIdx.x] = x;
-        sync();
-        long long r = 0;
-        const volatile long long* pp = G.partl + phase * gridDim.x;
-        for (unsigned k = 0; k < gridDim.x; ++k) r += pp[k];
-        phase ^= 1;
-        return r;
+        return greduce<long long>(x, G.partl, 0LL, [](long long a, long long b) { return a + b; });
     }
     __device__ long long gmax_ll(long long x) {
         x = block_max_ll<kGT>(x, sredl);
-        if (threadIdx.x == 0) G.partl[phase * gridDim.x + blockIdx.x] = x;
-        sync();
-        long long r = LLONG_MIN;
-        const volatile long long* pp = G.partl + phase * gridDim.x;
-        for (unsigned k = 0; k < gridDim.x; ++k) r = ::max(r, pp[k]);
-        phase ^= 1;
-        return r;
+        return greduce<long long>(x, G.partl, LLONG_MIN,
+                                  [](long long a, long long b) { return a > b ? a : b; });
     }
 
     __device__ __forceinline__ const volatile double* hc() const { return Hc; }
@@ -371,6 +370,7 @@ __global__ void __launch_bounds__(kGT) k_solve_grid(Batch B, DevParams P, GridSt
     __shared__ double sred[kGT / 32];
     __shared__ long long sredl[kGT / 32];
     __shared__ int swarp[kGT / 32 + 1];
+    __shared__ unsigned long long sbc[1];
     const Inst I = make_inst(B, b);
     const int V = I.V;
     const int v0 = (int)(((long long)V * blockIdx.x) / gridDim.x);
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(kGT) k_solve_grid(Batch B, DevParams P, GridSt
     const size_t head = (((size_t)nv + 1) * 4 + 15) / 16 * 16;
     double* eD = reinterpret_cast<double*>(smem_raw + head);
     uint32_t* eW = reinterpret_cast<uint32_t*>(eD + cap);
-    GridSolver S{B, P, G, I, b, v0, v1, I.row[0], G.Ha, G.Hb, eD, eW, cap, sefo, sred, sredl, swarp};
+    GridSolver S{B, P, G, I, b, v0, v1, I.row[0], G.Ha, G.Hb, eD, eW, cap, sefo, sred, sredl, swarp, sbc};
     double M;
     if (!refit) {
         for (int v = v0 + threadIdx.x; v < v1; v += kGT) G.Ha[v] = 0.0;  // F = 0

@@ -15,7 +15,9 @@
 #include <fstream>
 #include <iomanip>
 #include <memory>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <numeric>
 #include <string>
 #include <unordered_map>
@@ -662,7 +664,12 @@ f2m_status h2d(f2m_ctx* ctx, T* dst, const std::vector<T>& v) {
 }
 
 // Pull instance b (device-built graph, node ids = de-duplicated input order).
-f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, bool with_keys) {
+// Copies instance b to the host.  `mu` (optional) serialises the stream work
+// when several host threads complete instances of one call.
+f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, bool with_keys,
+                         std::mutex* mu = nullptr) {
+    std::unique_lock<std::mutex> lk;
+    if (mu) lk = std::unique_lock<std::mutex>(*mu);
     const Batch& B = C.B;
     int32_t V = 0;
     int64_t base = 0;
@@ -695,6 +702,7 @@ f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, boo
         if ((s = d2h(ctx, oth, B.s_oth + s0, S))) return s;
     }
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (lk.owns_lock()) lk.unlock();
     H.nbr.resize(S);
     H.Dn.resize(S);
     for (int64_t a = 0; a < S; ++a) { H.nbr[a] = sl[a].nbr; H.Dn[a] = sl[a].D; }
@@ -707,13 +715,18 @@ f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, boo
 
 // graph::RUN after the descent (graph_cuda.cu:64-153) for one instance:
 // host comb check, repair loop through device refits, primal and report values.
-f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& prm, f2m_result& R) {
+f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& prm, f2m_result& R,
+                             std::mutex* mu = nullptr) {
     HostInst& H = R.H;
     const double vb = prm.error_B * prm.error_B_comb;
     HostCheck HC(H, vb);
     int IRR_B = HC.check();
     int steps = 0;
     if (IRR_B > 0) {
+        // the repair steps use the call's stream and work lists: one host
+        // thread at a time
+        std::unique_lock<std::mutex> lk;
+        if (mu) lk = std::unique_lock<std::mutex>(*mu);
         int64_t ibase = 0, s0 = 0;
         F2M_CUDA(cudaMemcpyAsync(&ibase, C.B.offs + b, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
         F2M_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -964,19 +977,40 @@ static f2m_status check_args(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, 
 }
 
 // Host completion of the batch instances whose combs need the Ax=b stage.
+// Instances whose combs need the host stage (comb_thread.cpp, Ax_b.cpp) are
+// completed by a pool of host threads; copies and repair refits on the GPU
+// are serialised by a mutex, the host comb checks run side by side.
 static f2m_status complete_batch(f2m_ctx* ctx, DevCall& C, const f2m_params& prm,
                                  std::vector<int32_t>& status, std::vector<double>& lp,
                                  std::vector<int32_t>* max_rank) {
-    for (int b = 0; b < C.pl.n_inst; ++b) {
-        if (status[b] != kNeedsHost) continue;
-        f2m_result R;
-        f2m_status s = pull_instance(ctx, C, b, R.H, true);
+    std::vector<int> todo;
+    for (int b = 0; b < C.pl.n_inst; ++b)
+        if (status[b] == kNeedsHost) todo.push_back(b);
+    if (todo.empty()) return F2M_OK;
+    std::mutex mu;
+    std::atomic<size_t> next{0};
+    std::vector<f2m_status> err(todo.size(), F2M_OK);
+    auto work = [&]() {
+        for (size_t k; (k = next.fetch_add(1)) < todo.size();) {
+            const int b = todo[k];
+            f2m_result R;
+            f2m_status s = pull_instance(ctx, C, b, R.H, true, &mu);
+            if (!s) s = complete_instance(ctx, C, b, prm, R, &mu);
+            err[k] = s;
+            if (s) continue;
+            status[b] = R.status;
+            lp[b] = R.lp;
+            if (max_rank) (*max_rank)[b] = R.max_rank;
+        }
+    };
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min(todo.size(), std::min<size_t>(hw, 32));
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    for (f2m_status s : err)
         if (s) return s;
-        if ((s = complete_instance(ctx, C, b, prm, R))) return s;
-        status[b] = R.status;
-        lp[b] = R.lp;
-        if (max_rank) (*max_rank)[b] = R.max_rank;
-    }
     return F2M_OK;
 }
 
@@ -1111,11 +1145,18 @@ f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, cons
     F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.X_in), x, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.Y_in), y, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     auto t0 = std::chrono::steady_clock::now();
+    F2M_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
     F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
+    F2M_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
     F2M_CUDA(launch_knn(C.B, C.scan, ctx->stream, &ctx->launches));
+    F2M_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
     C.B.K_in = nullptr;
     F2M_CUDA(launch_graph(C.B, C.deg, C.scan, ctx->stream, &ctx->launches));
+    F2M_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
     if ((s = launch_classes(ctx, C, prm))) return s;
+    F2M_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
+    ctx->timed = true;
+    ctx->last = C.B;
     int32_t st = 0;
     F2M_CUDA(cudaMemcpyAsync(&st, C.B.status, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
