@@ -106,12 +106,23 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
+def sample_size(offs, x, y, threads, target_s):
+    """Instances (spread evenly over the batch) that keep the CPU busy for
+    about target_s seconds: grow a pilot sample until it takes a quarter of
+    that, then extrapolate (at most the whole batch)."""
+    total = len(offs) - 1
+    n = min(total, 4 * threads)
+    while True:
+        _, _, dt = run_cpu(offs, x, y, cpu_sample(offs, n), threads)
+        if dt >= target_s / 4 or n >= total:
+            break
+        n = min(total, 4 * n)
+    return int(min(total, max(n, n * target_s / max(dt, 1e-3))))
+
+
 def cpu_baseline(offs, x, y, target_s=15.0):
     threads = cpu_threads()
-    n = 16
-    idx = cpu_sample(offs, n)
-    _, _, dt = run_cpu(offs, x, y, idx, threads)
-    n = int(min(len(offs) - 1, max(16, n * target_s / max(dt, 1e-3))))
+    n = sample_size(offs, x, y, threads, target_s)
     idx = cpu_sample(offs, n)
     lp, st, dt = run_cpu(offs, x, y, idx, threads)
     return {"value": len(idx) / dt, "unit": "solves/s", "cores": threads, "kind": "port",
@@ -206,8 +217,8 @@ def reference_arm(args, rank, world):
         return
     offs, x, y = workload(0, args.n_inst)
     threads = cpu_threads()
-    n_sample = int(min(args.n_inst, max(32, 4 * threads)))
-    idx = cpu_sample(offs, n_sample)
+    # each step is a bounded sample (about 5 s of CPU work) of the same batch
+    idx = cpu_sample(offs, sample_size(offs, x, y, threads, 5.0))
     for _ in range(args.warmup):
         run_cpu(offs, x, y, idx[: max(4, len(idx) // 8)], threads)
     times = []
