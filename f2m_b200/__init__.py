@@ -75,6 +75,11 @@ class BatchOut(ctypes.Structure):
                 ("iterations", ctypes.c_void_p)]
 
 
+class SmoothParams(ctypes.Structure):
+    _fields_ = [("tau", ctypes.c_double), ("iters", ctypes.c_int32), ("damping", ctypes.c_double),
+                ("newton_max", ctypes.c_int32), ("checkpoint", ctypes.c_int32)]
+
+
 # Every symbol include/f2m.h declares.
 EXPORTS = [
     "f2m_default_params", "f2m_create", "f2m_destroy", "f2m_last_error", "f2m_kernel_launches",
@@ -82,7 +87,8 @@ EXPORTS = [
     "f2m_solve_file", "f2m_result_free", "f2m_result_status", "f2m_result_n_nodes",
     "f2m_result_n_edges", "f2m_result_lp", "f2m_result_max_rank", "f2m_result_seconds",
     "f2m_result_edges", "f2m_result_nodes", "f2m_result_stats", "f2m_phase_times",
-    "f2m_solve_points_noalloc",
+    "f2m_solve_points_noalloc", "f2m_default_smooth_params", "f2m_smoothed_bound_fwd",
+    "f2m_smoothed_bound_bwd", "f2m_smooth_max_nodes",
 ]
 
 _lib = None
@@ -122,6 +128,11 @@ def lib():
         L.f2m_result_stats.argtypes = [vp, P(Stats)]
         L.f2m_phase_times.argtypes = [vp, vp, P(Work)]
         L.f2m_solve_points_noalloc.argtypes = [vp, vp, i32, i32, P(Params), vp, vp, vp]
+        L.f2m_default_smooth_params.argtypes = [P(SmoothParams)]
+        L.f2m_smoothed_bound_fwd.argtypes = [vp, i32, vp, vp, vp, i32, P(SmoothParams), vp]
+        L.f2m_smoothed_bound_bwd.argtypes = [vp, i32, vp, vp, vp, i32, P(SmoothParams), vp, vp,
+                                             vp, vp]
+        L.f2m_smooth_max_nodes.restype = i32
         _lib = L
     return _lib
 
@@ -129,6 +140,14 @@ def lib():
 def default_params(**overrides):
     p = Params()
     lib().f2m_default_params(ctypes.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def default_smooth_params(**overrides):
+    p = SmoothParams()
+    lib().f2m_default_smooth_params(ctypes.byref(p))
     for k, v in overrides.items():
         setattr(p, k, v)
     return p
@@ -222,6 +241,28 @@ class Context:
         return ms, {k: getattr(w, k) for k, _ in Work._fields_}
 
     # -- single instance ----------------------------------------------------
+    # -- smoothed bound (no counterpart in the reference) ------------------
+    def smoothed_bound(self, offs, x, y, top_k, params=None, grad=False, dL=None):
+        """Smoothed F2M dual bound per instance (FP32 points); with grad=True
+        also d(sum_b dL[b] L[b]) / d(x, y).  Returns L or (L, dL_dx, dL_dy)."""
+        offs = np.ascontiguousarray(offs, np.int64)
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        n = len(offs) - 1
+        p = params if params is not None else default_smooth_params()
+        L = np.zeros(n, np.float64)
+        if not grad:
+            self._check(lib().f2m_smoothed_bound_fwd(self._h, n, _ptr(offs), _ptr(x), _ptr(y), top_k,
+                                                     ctypes.byref(p), _ptr(L)))
+            return L
+        gx = np.zeros(len(x), np.float32)
+        gy = np.zeros(len(y), np.float32)
+        up = None if dL is None else np.ascontiguousarray(dL, np.float64)
+        self._check(lib().f2m_smoothed_bound_bwd(self._h, n, _ptr(offs), _ptr(x), _ptr(y), top_k,
+                                                 ctypes.byref(p), _ptr(up), _ptr(L), _ptr(gx),
+                                                 _ptr(gy)))
+        return L, gx, gy
+
     def solve_points(self, x, y, top_k, labels=None, params=None):
         x = np.ascontiguousarray(x, np.float64)
         y = np.ascontiguousarray(y, np.float64)

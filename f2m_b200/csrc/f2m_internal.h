@@ -153,6 +153,45 @@ cudaError_t launch_refit_class(int c, const Batch& B, const DevParams& P, const 
                                int64_t* launches);
 int solve_num_classes();
 int solve_class_of(int32_t n);
+// Smoothed-bound batch (f2m_smooth.cu).  Node g of instance b is offs[b] +
+// local id; neighbour ids in nbr are local; slots are global (row).
+struct SmoothBatch {
+    int32_t n_inst = 0, N = 0;
+    int64_t n_total = 0;
+    const int64_t* offs = nullptr;
+    const float* x = nullptr;
+    const float* y = nullptr;
+    unsigned long long* top = nullptr;  // [n_total * N] (cost bits << 32 | local index)
+    int32_t* rdeg = nullptr;            // [n_total]
+    int32_t* tcur = nullptr;            // [n_total]
+    int64_t* tcap = nullptr;            // [n_total + 1] temporary list offsets
+    int32_t* tnbr = nullptr;            // [2 * n_total * N]
+    int64_t* deg = nullptr;             // [n_total] scan input
+    int64_t* row = nullptr;             // [n_total + 1]
+    int32_t* nbr = nullptr;             // [S]
+    int64_t* mirror = nullptr;          // [S] slot of the same edge in the neighbour's list
+    float* c = nullptr;                 // [S]
+    double tau = 0, omega = 0;
+    int32_t iters = 0, newton_max = 0, ckpt = 1, n_ck = 1;
+    double* L = nullptr;                // [n_inst]
+    const double* dL = nullptr;         // [n_inst] upstream gradient
+    double* ck = nullptr;               // [n_total * n_ck] checkpoints of u
+    double* segu = nullptr;             // [n_total * ckpt] recomputed iterates
+    double* segs = nullptr;             // [n_total * ckpt] their roots
+    double* lam = nullptr;              // [n_total]
+    double* lam2 = nullptr;             // [n_total]
+    double* q = nullptr;                // [S]
+    double* gc = nullptr;               // [S] dL/dc accumulated per slot
+    float* gx = nullptr;                // [n_total]
+    float* gy = nullptr;                // [n_total]
+    int32_t* queue = nullptr;
+};
+cudaError_t launch_smooth_graph(SmoothBatch& S, int64_t* scan_scratch, cudaStream_t s,
+                                int64_t* launches);
+cudaError_t launch_smooth_bound(SmoothBatch& S, int32_t max_v, bool grad, cudaStream_t s,
+                                int64_t* launches);
+int32_t smooth_max_nodes();
+
 cudaError_t launch_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* scratch,
                         cudaStream_t s, int64_t* launches);
 int64_t scan_scratch_elems(int64_t n);

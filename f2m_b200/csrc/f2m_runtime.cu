@@ -1176,6 +1176,135 @@ f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, cons
     return (f2m_status)(*out)->status;
 }
 
+/* ------------------------------------------------------------------ */
+/* smoothed bound (f2m_smooth.cu)                                       */
+/* ------------------------------------------------------------------ */
+void f2m_default_smooth_params(f2m_smooth_params* p) {
+    p->tau = 1e-3;
+    p->iters = 100;
+    p->damping = 0.5;
+    p->newton_max = 60;
+    p->checkpoint = 16;
+}
+
+int32_t f2m_smooth_max_nodes(void) { return smooth_max_nodes(); }
+
+}  // extern "C"
+
+namespace {
+
+// Shared body of the smoothed-bound entry points: buffers from the context's
+// arena, host inputs copied in, graph + bound (+ adjoint) on the device.
+f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const float* x,
+                       const float* y, int32_t top_k, const f2m_smooth_params* p,
+                       const double* dL, double* L, float* gx, float* gy) {
+    if (!ctx) return F2M_ERR_INPUT;
+    if (n_inst < 1 || !offs || !x || !y || !L) return fail(ctx, F2M_ERR_INPUT, "missing inputs");
+    if (top_k < 3 || top_k > 64) return fail(ctx, F2M_ERR_INPUT, "top_k must be in [3, 64]");
+    f2m_smooth_params sp;
+    f2m_default_smooth_params(&sp);
+    if (p) sp = *p;
+    if (!(sp.tau > 0) || sp.iters < 0 || !(sp.damping > 0 && sp.damping <= 1) || sp.newton_max < 1 ||
+        sp.checkpoint < 1)
+        return fail(ctx, F2M_ERR_INPUT, "invalid smoothing parameters");
+    if (offs[0] != 0) return fail(ctx, F2M_ERR_INPUT, "offs[0] must be 0");
+    cudaSetDevice(ctx->device);
+    const int32_t vmax = smooth_max_nodes();
+    int32_t max_v = 0;
+    for (int32_t b = 0; b < n_inst; ++b) {
+        const int64_t v = offs[b + 1] - offs[b];
+        if (v < 4) return fail(ctx, F2M_ERR_INPUT, "every instance needs at least 4 points");
+        if (v > vmax)
+            return fail(ctx, F2M_ERR_CAPACITY, "instances are limited to " + std::to_string(vmax) + " points");
+        max_v = std::max<int32_t>(max_v, (int32_t)v);
+    }
+    const int64_t n = offs[n_inst];
+    const bool grad = gx || gy;
+    const int32_t N = top_k;
+    const int32_t K = sp.checkpoint;
+    const int32_t nck = std::max(1, (sp.iters + K - 1) / K);
+    const int64_t S = 2 * n * N;
+    SmoothBatch B;
+    int64_t* scan = nullptr;
+    double* dLd = nullptr;
+    auto carve_s = [&](Arena& A) {
+        B.offs = A.take<int64_t>(n_inst + 1);
+        B.x = A.take<float>(n);
+        B.y = A.take<float>(n);
+        B.top = A.take<unsigned long long>(n * N);
+        B.rdeg = A.take<int32_t>(n);
+        B.tcur = A.take<int32_t>(n);
+        B.tcap = A.take<int64_t>(n + 1);
+        B.tnbr = A.take<int32_t>(S);
+        B.deg = A.take<int64_t>(n);
+        B.row = A.take<int64_t>(n + 1);
+        scan = A.take<int64_t>(scan_scratch_elems(n) + 1);
+        B.nbr = A.take<int32_t>(S);
+        B.mirror = A.take<int64_t>(S);
+        B.c = A.take<float>(S);
+        B.L = A.take<double>(n_inst);
+        dLd = A.take<double>(n_inst);
+        B.queue = A.take<int32_t>(1);
+        if (grad) {
+            B.ck = A.take<double>(n * nck);
+            B.segu = A.take<double>(n * K);
+            B.segs = A.take<double>(n * K);
+            B.lam = A.take<double>(n);
+            B.lam2 = A.take<double>(n);
+            B.q = A.take<double>(S);
+            B.gc = A.take<double>(S);
+            B.gx = A.take<float>(n);
+            B.gy = A.take<float>(n);
+        }
+    };
+    Arena A;
+    carve_s(A);
+    F2M_CUDA(ensure_device(ctx, A.used));
+    A.base = ctx->dev;
+    A.used = 0;
+    carve_s(A);
+    ctx->timed = false;  // the arena no longer holds a solve batch
+    B.n_inst = n_inst;
+    B.N = N;
+    B.n_total = n;
+    B.tau = sp.tau;
+    B.omega = sp.damping;
+    B.iters = sp.iters;
+    B.newton_max = sp.newton_max;
+    B.ckpt = K;
+    B.n_ck = nck;
+    B.dL = dLd;
+    std::vector<double> up(n_inst, 1.0);
+    if (dL) std::copy(dL, dL + n_inst, up.begin());
+    F2M_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(B.offs), offs, (n_inst + 1) * sizeof(int64_t),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<float*>(B.x), x, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(const_cast<float*>(B.y), y, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(dLd, up.data(), n_inst * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    F2M_CUDA(launch_smooth_graph(B, scan, ctx->stream, &ctx->launches));
+    F2M_CUDA(launch_smooth_bound(B, max_v, grad, ctx->stream, &ctx->launches));
+    F2M_CUDA(cudaMemcpyAsync(L, B.L, n_inst * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (gx) F2M_CUDA(cudaMemcpyAsync(gx, B.gx, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    if (gy) F2M_CUDA(cudaMemcpyAsync(gy, B.gy, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    return F2M_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+f2m_status f2m_smoothed_bound_fwd(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const float* x,
+                                  const float* y, int32_t top_k, const f2m_smooth_params* p, double* L) {
+    return smooth_call(ctx, n_inst, offs, x, y, top_k, p, nullptr, L, nullptr, nullptr);
+}
+
+f2m_status f2m_smoothed_bound_bwd(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const float* x,
+                                  const float* y, int32_t top_k, const f2m_smooth_params* p,
+                                  const double* dL, double* L, float* dL_dx, float* dL_dy) {
+    if (!dL_dx || !dL_dy) return ctx ? fail(ctx, F2M_ERR_INPUT, "dL_dx and dL_dy are required") : F2M_ERR_INPUT;
+    return smooth_call(ctx, n_inst, offs, x, y, top_k, p, dL, L, dL_dx, dL_dy);
+}
 
 }  // extern "C"
 

@@ -9,6 +9,10 @@ value(seed, stream, i) = splitmix64(seed * 2**32 + stream * 2**24 + i).
            rounded and clamped to integers
   config3: 4,096 instances, sizes log-uniform in [50, 5000], integer
            coordinates uniform in [0, 10^4)^2
+  config4: 10,000 FP32 points uniform in [0, 1)^2 (smoothed bound)
+  config5: 1,024 instances, sizes uniform in [200, 2000], FP32 points on a
+           jittered unit square lattice (jitter uniform in +-0.3) (smoothed
+           bound, batched)
 """
 import numpy as np
 
@@ -78,6 +82,35 @@ def config3(seed=3, n_inst=4096, lo=50, hi=5000, box=10_000):
     x = np.floor(uniform(seed, 101, n) * box)
     y = np.floor(uniform(seed, 102, n) * box)
     return offs, x, y
+
+
+def config4(seed=4, n=10_000):
+    x = uniform(seed, 300, n).astype(np.float32)
+    y = uniform(seed, 301, n).astype(np.float32)
+    return x, y
+
+
+def jittered_lattice(n, seed, stream=310, jitter=0.3):
+    """n FP32 points: the first n sites of a square unit lattice (row-major,
+    side ceil(sqrt n)), each moved by a uniform offset in +-jitter."""
+    side = int(np.ceil(np.sqrt(n)))
+    i = np.arange(n)
+    x = (i % side) + (2 * uniform(seed, stream, n) - 1) * jitter
+    y = (i // side) + (2 * uniform(seed, stream + 1, n) - 1) * jitter
+    return x.astype(np.float32), y.astype(np.float32)
+
+
+def config5(seed=5, n_inst=1024, lo=200, hi=2000):
+    """(offs, x, y) of n_inst jittered-lattice instances."""
+    sizes = lo + np.floor(uniform(seed, 320, n_inst) * (hi - lo + 1)).astype(np.int64)
+    offs = np.zeros(n_inst + 1, np.int64)
+    offs[1:] = np.cumsum(sizes)
+    xs, ys = [], []
+    for b in range(n_inst):
+        x, y = jittered_lattice(int(sizes[b]), seed * 100_000 + b)
+        xs.append(x)
+        ys.append(y)
+    return offs, np.concatenate(xs), np.concatenate(ys)
 
 
 def lattice_points(n, seed, side=None, keep=0.7):

@@ -200,6 +200,40 @@ typedef struct f2m_stats {
 } f2m_stats;
 void f2m_result_stats(const f2m_result* r, f2m_stats* s);
 
+/* ------------------------------------------------------------------------
+ * Entropically smoothed F2M dual bound and its gradient.  No counterpart in
+ * the reference (it solves the LP only); this is the differentiable
+ * extension of the same method.  Per instance: the graph is the union of
+ * each point's top_k nearest neighbours by FP32 Euclidean distance (ties by
+ * index, no rounding or de-duplication); with z_e = (u_a + u_b - c_e)/tau,
+ *   L(u) = 2 sum_v u_v - tau sum_e softplus(z_e)
+ * bounds the entropy-smoothed fractional 2-matching LP from below for every
+ * u.  u comes from `iters` damped Jacobi coordinate-ascent steps from 0; the
+ * gradient is the exact adjoint of that computation (iterates recomputed
+ * from checkpoints every `checkpoint` steps), chained through c_e = |p_a-p_b|.
+ * At a stationary u, dL/dc_e = sigmoid(z_e), the smoothed x_e. */
+typedef struct f2m_smooth_params {
+    double tau;          /* temperature (> 0) */
+    int32_t iters;       /* Jacobi steps (>= 0) */
+    double damping;      /* omega in (0, 1]: u <- (1-omega) u + omega root */
+    int32_t newton_max;  /* Newton steps per node root */
+    int32_t checkpoint;  /* steps between stored iterates in the backward pass */
+} f2m_smooth_params;
+void f2m_default_smooth_params(f2m_smooth_params* p); /* 1e-3, 100, 0.5, 60, 16 */
+
+/* Forward: L[b] for each instance (offs has n_inst+1 entries into x/y, host
+ * arrays; 3 <= top_k <= 64; at most f2m_smooth_max_nodes() points each). */
+f2m_status f2m_smoothed_bound_fwd(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs,
+                                  const float* x, const float* y, int32_t top_k,
+                                  const f2m_smooth_params* p, double* L);
+/* Backward: recomputes the forward pass, writes L and the gradient of
+ * sum_b dL[b] * L[b] with respect to the coordinates (dL null = all ones). */
+f2m_status f2m_smoothed_bound_bwd(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs,
+                                  const float* x, const float* y, int32_t top_k,
+                                  const f2m_smooth_params* p, const double* dL, double* L,
+                                  float* dL_dx, float* dL_dy);
+int32_t f2m_smooth_max_nodes(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -112,6 +112,20 @@ int orc_solve_batch(int32_t n_inst, const int64_t* offs, const double* X,
                     const double* Y, int top_k, int cost_mode, int threads,
                     double* lp_out, int32_t* status_out, int64_t* iters_out);
 
+/* Entropically smoothed F2M dual bound (f2m_smooth_oracle.cpp).  Graph of
+ * the FP32 points: union of each point's top_k nearest (ties by index), lists
+ * ascending in neighbour index.  orc_smooth_graph fills row (n+1) and, when
+ * cap >= S, nbr/c (S); returns S. */
+int orc_smooth_graph(const float* x, const float* y, int32_t n, int32_t top_k, int64_t* row,
+                     int32_t* nbr, float* c, int64_t cap);
+/* L = bound after `iters` damped Jacobi steps; dLdx/dLdy (n) and dLdc (S,
+ * per slot, the edge's total) when non-null.  Graph from (gx, gy) if given;
+ * costs from (x, y) on that graph, or c_override. */
+int orc_smooth_bound(const float* x, const float* y, int32_t n, int32_t top_k, double tau,
+                     int32_t iters, double omega, int32_t newton_max, const float* gx,
+                     const float* gy, const float* c_override, double* L, double* dLdx,
+                     double* dLdy, double* dLdc);
+
 #ifdef __cplusplus
 }
 #endif

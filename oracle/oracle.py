@@ -85,6 +85,11 @@ def lib():
         L.orc_get_cutoffs.argtypes = [vp, vp, vp]
         L.orc_solve_batch.argtypes = [ctypes.c_int32, vp, vp, vp, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int, vp, vp, vp]
+        L.orc_smooth_graph.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp,
+                                       ctypes.c_int64]
+        L.orc_smooth_bound.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                       ctypes.c_int32, ctypes.c_double, ctypes.c_int32, vp, vp,
+                                       vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -207,3 +212,43 @@ def solve_batch(offs, X, Y, top_k, cost=COST_REF, threads=1):
     lib().orc_solve_batch(n, _ptr(offs), _ptr(X), _ptr(Y), top_k, cost, threads, _ptr(lp),
                           _ptr(status), _ptr(iters))
     return lp, status, iters
+
+
+# -- smoothed bound (f2m_smooth_oracle.cpp) ----------------------------------
+def smooth_graph(x, y, top_k):
+    """(row, nbr, c) of the FP32 kNN union graph of one instance."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    n = len(x)
+    row = np.zeros(n + 1, np.int64)
+    S = lib().orc_smooth_graph(_ptr(x), _ptr(y), n, top_k, _ptr(row), None, None, 0)
+    nbr = np.zeros(S, np.int32)
+    c = np.zeros(S, np.float32)
+    lib().orc_smooth_graph(_ptr(x), _ptr(y), n, top_k, _ptr(row), _ptr(nbr), _ptr(c), S)
+    return row, nbr, c
+
+
+def smooth_bound(x, y, top_k, tau=1e-3, iters=100, omega=0.5, newton_max=60, grad=False,
+                 graph_xy=None, c=None):
+    """FP64 host bound of one instance; with grad=True returns (L, dLdx, dLdy,
+    dLdc).  graph_xy fixes the graph (points it is built from); c replaces the
+    edge costs (per slot)."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    n = len(x)
+    gx = gy = None
+    if graph_xy is not None:
+        gx = np.ascontiguousarray(graph_xy[0], np.float32)
+        gy = np.ascontiguousarray(graph_xy[1], np.float32)
+    co = None if c is None else np.ascontiguousarray(c, np.float32)
+    L = ctypes.c_double()
+    dx = dy = dc = None
+    if grad:
+        S = int(smooth_graph(gx if gx is not None else x, gy if gy is not None else y, top_k)[1].size)
+        dx, dy, dc = np.zeros(n), np.zeros(n), np.zeros(S)
+    st = lib().orc_smooth_bound(_ptr(x), _ptr(y), n, top_k, tau, iters, omega, newton_max,
+                                _ptr(gx), _ptr(gy), _ptr(co), ctypes.byref(L), _ptr(dx), _ptr(dy),
+                                _ptr(dc))
+    if st != OK:
+        raise ValueError(f"orc_smooth_bound status {st}")
+    return (L.value, dx, dy, dc) if grad else L.value

@@ -1,0 +1,120 @@
+"""Smoothed F2M dual bound and its adjoint (no reference counterpart).
+
+CPU suite: the FP64 host oracle (oracle/f2m_smooth_oracle.cpp) against
+central finite differences on a fixed graph.  GPU suite (through the C ABI):
+the CUDA forward and adjoint against the FP64 host gradient, on single
+instances and a batch."""
+import numpy as np
+import pytest
+
+from f2m_b200 import synth
+
+TAU = 1e-3
+FD_STEP = 1e-4
+
+
+def _fd_points(n, seed):
+    x, y = synth.config4(seed, n)
+    return x, y
+
+
+def test_oracle_gradient_matches_central_differences():
+    """FD step 1e-4 on seeded coordinates; the graph is held fixed."""
+    from oracle import oracle as O
+    x, y = _fd_points(400, 7)
+    N, iters = 12, 40
+    L0, dx, dy, _ = O.smooth_bound(x, y, N, tau=TAU, iters=iters, grad=True)
+    rng = np.random.default_rng(3)
+    idx = rng.choice(len(x), 16, replace=False)
+    for i in idx:
+        for arr, g in ((x, dx), (y, dy)):
+            p, m = arr.copy(), arr.copy()
+            p[i] = np.float32(arr[i] + FD_STEP)
+            m[i] = np.float32(arr[i] - FD_STEP)
+            h = float(p[i]) - float(m[i])
+            xp, yp = (p, y) if arr is x else (x, p)
+            xm, ym = (m, y) if arr is x else (x, m)
+            Lp = O.smooth_bound(xp, yp, N, tau=TAU, iters=iters, graph_xy=(x, y))
+            Lm = O.smooth_bound(xm, ym, N, tau=TAU, iters=iters, graph_xy=(x, y))
+            fd = (Lp - Lm) / h
+            assert abs(fd - g[i]) <= 2e-3 * max(1.0, abs(g[i])), (i, fd, g[i])
+
+
+def test_oracle_cost_gradient_is_smoothed_x_at_stationarity():
+    """With enough steps u is stationary and dL/dc_e -> sigmoid(z_e), the
+    smoothed primal, whose node sums are 2."""
+    from oracle import oracle as O
+    x, y = _fd_points(200, 11)
+    N = 8
+    row, nbr, c = O.smooth_graph(x, y, N)
+    _, _, _, dc = O.smooth_bound(x, y, N, tau=1e-2, iters=400, omega=0.5, grad=True)
+    deg = np.add.reduceat(dc, row[:-1])
+    assert np.allclose(deg, 2.0, atol=1e-6)
+    assert np.all(dc >= -1e-9) and np.all(dc <= 1 + 1e-9)
+
+
+@pytest.mark.gpu
+def test_cuda_graph_and_bound_match_oracle(ctx):
+    from oracle import oracle as O
+    import f2m_b200
+    x, y = synth.config4(4, 3000)
+    N, iters = 30, 60
+    p = f2m_b200.default_smooth_params(tau=TAU, iters=iters)
+    offs = np.array([0, len(x)], np.int64)
+    L, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
+    Lo, dx, dy, _ = O.smooth_bound(x, y, N, tau=TAU, iters=iters, grad=True)
+    assert abs(L[0] - Lo) <= 1e-9 * abs(Lo)
+    scale = max(np.abs(dx).max(), np.abs(dy).max())
+    assert np.abs(gx - dx).max() <= 1e-5 * scale
+    assert np.abs(gy - dy).max() <= 1e-5 * scale
+    Lf = ctx.smoothed_bound(offs, x, y, N, params=p)
+    assert Lf[0] == L[0]
+
+
+@pytest.mark.gpu
+def test_cuda_batch_forward_adjoint_matches_oracle(ctx):
+    """Jittered-lattice batch (the batched smoothed configuration, 24
+    instances), with per-instance upstream gradients."""
+    from oracle import oracle as O
+    import f2m_b200
+    offs, x, y = synth.config5(5, n_inst=24, lo=200, hi=600)
+    N, iters = 24, 40
+    p = f2m_b200.default_smooth_params(tau=TAU, iters=iters, checkpoint=7)
+    up = 1.0 + np.arange(24) / 10
+    L, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True, dL=up)
+    for b in range(24):
+        s, e = offs[b], offs[b + 1]
+        Lo, dx, dy, _ = O.smooth_bound(x[s:e], y[s:e], N, tau=TAU, iters=iters, grad=True)
+        assert abs(L[b] - Lo) <= 1e-9 * abs(Lo), b
+        scale = max(np.abs(dx).max(), np.abs(dy).max()) * up[b]
+        assert np.abs(gx[s:e] - up[b] * dx).max() <= 1e-5 * scale, b
+        assert np.abs(gy[s:e] - up[b] * dy).max() <= 1e-5 * scale, b
+
+
+@pytest.mark.gpu
+def test_cuda_gradient_matches_central_differences(ctx):
+    """Config-4 shape (10,000 points, N=30, tau=1e-3): CUDA gradient against
+    central differences of the FP64 host bound (step 1e-4, graph fixed) on
+    seeded coordinates."""
+    from oracle import oracle as O
+    import f2m_b200
+    x, y = synth.config4(4)
+    N, iters = 30, 30
+    p = f2m_b200.default_smooth_params(tau=TAU, iters=iters)
+    offs = np.array([0, len(x)], np.int64)
+    _, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
+    rng = np.random.default_rng(128)
+    for i in rng.choice(len(x), 8, replace=False):
+        p_, m_ = x.copy(), x.copy()
+        p_[i] = np.float32(x[i] + FD_STEP)
+        m_[i] = np.float32(x[i] - FD_STEP)
+        Lp = O.smooth_bound(p_, y, N, tau=TAU, iters=iters, graph_xy=(x, y))
+        Lm = O.smooth_bound(m_, y, N, tau=TAU, iters=iters, graph_xy=(x, y))
+        fd = (Lp - Lm) / (float(p_[i]) - float(m_[i]))
+        assert abs(fd - gx[i]) <= 5e-3 * max(1.0, abs(gx[i])), (i, fd, gx[i])
+
+
+def test_smooth_input_errors_without_device():
+    import f2m_b200
+    with pytest.raises(f2m_b200.F2MError):
+        f2m_b200.Context(0).smoothed_bound(np.array([0, 3]), np.zeros(3), np.zeros(3), 3)
