@@ -42,10 +42,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["batch", "large"],
+    ap.add_argument("--workload", default="batch", choices=["batch", "large", "smooth", "smooth1"],
                     help="batch: 4,096 mixed-size instances (the headline); large: one "
-                         "100,000-point Gaussian-mixture instance with N=50 (grid-wide solver)")
+                         "100,000-point Gaussian-mixture instance with N=50 (grid-wide solver); "
+                         "smooth: smoothed bound + adjoint of 1,024 jittered-lattice instances "
+                         "(N=24); smooth1: the same on 10,000 uniform FP32 points (N=30)")
     ap.add_argument("--large-n", type=int, default=100_000, help="points of the large instance")
+    ap.add_argument("--smooth-solver", type=int, default=0, choices=[0, 1, 2],
+                    help="smoothed bound: 0 auto, 1 one CTA per instance, 2 one launch per step")
     ap.add_argument("--n-inst", type=int, default=N_INST)
     ap.add_argument("--plain-sample", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -441,6 +445,62 @@ def large_arm(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def smooth_arm(args, rank, world, local_rank):
+    """Smoothed bound + adjoint (tau = 1e-3, 100 damped Jacobi steps,
+    checkpoints every 16): `smooth` = 1,024 jittered-lattice instances of
+    200-2,000 points (N=24), `smooth1` = 10,000 uniform FP32 points (N=30).
+    Host arrays in and out through the C ABI (the entry points copy)."""
+    import torch
+
+    import f2m_b200
+    torch.cuda.set_device(local_rank)
+    if args.workload == "smooth":
+        offs, x, y = synth.config5(5 + rank)
+        N, desc = 24, "1,024 instances, sizes uniform in [200,2000], jittered unit lattice (+-0.3), FP32"
+    else:
+        x, y = synth.config4(4 + rank)
+        offs, N, desc = np.array([0, len(x)], np.int64), 30, "10,000 FP32 points uniform in [0,1)^2"
+    n_inst = len(offs) - 1
+    ctx = f2m_b200.Context(local_rank)
+    p = f2m_b200.default_smooth_params(solver=args.smooth_solver)
+    for _ in range(args.warmup):
+        ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
+    clk = Clocks(local_rank)
+    l0 = ctx.kernel_launches()
+    ms = []
+    clk.start()
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
+        ms.append(1e3 * (time.perf_counter() - t0))
+    clocks = clk.stop()
+    launches = ctx.kernel_launches() - l0
+    t = float(np.mean(ms))
+    if world > 1:
+        tt = torch.tensor([t], dtype=torch.float64, device=torch.device("cuda", local_rank))
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t = float(tt.item())
+    if rank != 0:
+        return
+    line = {
+        "metric": "smoothed F2M bound + coordinate gradient, instances/s", "value": n_inst * world / (t / 1e3),
+        "unit": "instances/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (FP32 coordinates)", "data": "synthetic (seeded)",
+        "config": {"workload": desc, "top_k": N, "tau": p.tau, "iters": p.iters,
+                   "damping": p.damping, "checkpoint": p.checkpoint,
+                   "parallelism": f"instance sharding over {world} GPU(s), no collective"},
+        "roofline": None,
+        "e2e": {"value": n_inst * world / (t / 1e3), "unit": "instances/s",
+                "h2d_bytes_per_step": int(offs.nbytes + x.nbytes + y.nbytes),
+                "d2h_bytes_per_step": int(L.nbytes + gx.nbytes + gy.nbytes)},
+        "clocks": clocks, "gpu_launches": int(launches // max(args.steps, 1)),
+        "L_mean": float(np.mean(L)), "grad_rms": float(np.sqrt(np.mean(gx.astype(np.float64) ** 2))),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -460,6 +520,8 @@ def main():
             reference_arm(args, rank, world)
         elif args.workload == "large":
             large_arm(args, rank, world, local_rank)
+        elif args.workload in ("smooth", "smooth1"):
+            smooth_arm(args, rank, world, local_rank)
         else:
             ours_arm(args, rank, world, local_rank)
     finally:

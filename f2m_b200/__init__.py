@@ -77,7 +77,8 @@ class BatchOut(ctypes.Structure):
 
 class SmoothParams(ctypes.Structure):
     _fields_ = [("tau", ctypes.c_double), ("iters", ctypes.c_int32), ("damping", ctypes.c_double),
-                ("newton_max", ctypes.c_int32), ("checkpoint", ctypes.c_int32)]
+                ("newton_max", ctypes.c_int32), ("checkpoint", ctypes.c_int32),
+                ("solver", ctypes.c_int32)]
 
 
 # Every symbol include/f2m.h declares.

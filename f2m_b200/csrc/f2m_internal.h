@@ -175,7 +175,11 @@ struct SmoothBatch {
     int32_t iters = 0, newton_max = 0, ckpt = 1, n_ck = 1;
     double* L = nullptr;                // [n_inst]
     const double* dL = nullptr;         // [n_inst] upstream gradient
+    int32_t solver = 0;                 // 1: one CTA per instance, 2: one launch per step
     double* ck = nullptr;               // [n_total * n_ck] checkpoints of u
+    double* ua = nullptr;               // [n_total] potentials (per-step path)
+    double* ub = nullptr;               // [n_total]
+    double* Lp = nullptr;               // [n_total] per-node terms of L (per-step path)
     double* segu = nullptr;             // [n_total * ckpt] recomputed iterates
     double* segs = nullptr;             // [n_total * ckpt] their roots
     double* lam = nullptr;              // [n_total]
@@ -190,6 +194,7 @@ cudaError_t launch_smooth_graph(SmoothBatch& S, int64_t* scan_scratch, cudaStrea
                                 int64_t* launches);
 cudaError_t launch_smooth_bound(SmoothBatch& S, int32_t max_v, bool grad, cudaStream_t s,
                                 int64_t* launches);
+cudaError_t launch_smooth_steps(SmoothBatch& S, bool grad, cudaStream_t s, int64_t* launches);
 int32_t smooth_max_nodes();
 
 cudaError_t launch_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* scratch,

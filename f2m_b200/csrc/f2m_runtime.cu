@@ -1185,6 +1185,7 @@ void f2m_default_smooth_params(f2m_smooth_params* p) {
     p->damping = 0.5;
     p->newton_max = 60;
     p->checkpoint = 16;
+    p->solver = 0;
 }
 
 int32_t f2m_smooth_max_nodes(void) { return smooth_max_nodes(); }
@@ -1205,7 +1206,7 @@ f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const 
     f2m_default_smooth_params(&sp);
     if (p) sp = *p;
     if (!(sp.tau > 0) || sp.iters < 0 || !(sp.damping > 0 && sp.damping <= 1) || sp.newton_max < 1 ||
-        sp.checkpoint < 1)
+        sp.checkpoint < 1 || sp.solver < 0 || sp.solver > 2)
         return fail(ctx, F2M_ERR_INPUT, "invalid smoothing parameters");
     if (offs[0] != 0) return fail(ctx, F2M_ERR_INPUT, "offs[0] must be 0");
     cudaSetDevice(ctx->device);
@@ -1223,7 +1224,8 @@ f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const 
     const int32_t N = top_k;
     const int32_t K = sp.checkpoint;
     const int32_t nck = std::max(1, (sp.iters + K - 1) / K);
-    const int64_t S = 2 * n * N;
+    const int64_t S = 2 * n * N + 8 * n;  // union lists: own N + reverse (+ slack)
+    const bool steps = sp.solver == 2 || (sp.solver == 0 && n_inst < ctx->sms);
     SmoothBatch B;
     int64_t* scan = nullptr;
     double* dLd = nullptr;
@@ -1245,6 +1247,11 @@ f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const 
         B.L = A.take<double>(n_inst);
         dLd = A.take<double>(n_inst);
         B.queue = A.take<int32_t>(1);
+        if (steps) {
+            B.ua = A.take<double>(n);
+            B.ub = A.take<double>(n);
+            B.Lp = A.take<double>(n);
+        }
         if (grad) {
             B.ck = A.take<double>(n * nck);
             B.segu = A.take<double>(n * K);
@@ -1282,7 +1289,9 @@ f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const 
     F2M_CUDA(cudaMemcpyAsync(const_cast<float*>(B.y), y, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(cudaMemcpyAsync(dLd, up.data(), n_inst * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(launch_smooth_graph(B, scan, ctx->stream, &ctx->launches));
-    F2M_CUDA(launch_smooth_bound(B, max_v, grad, ctx->stream, &ctx->launches));
+    B.solver = steps ? 2 : 1;
+    if (steps) F2M_CUDA(launch_smooth_steps(B, grad, ctx->stream, &ctx->launches));
+    else F2M_CUDA(launch_smooth_bound(B, max_v, grad, ctx->stream, &ctx->launches));
     F2M_CUDA(cudaMemcpyAsync(L, B.L, n_inst * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (gx) F2M_CUDA(cudaMemcpyAsync(gx, B.gx, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     if (gy) F2M_CUDA(cudaMemcpyAsync(gy, B.gy, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));

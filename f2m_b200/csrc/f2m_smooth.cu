@@ -178,35 +178,55 @@ __device__ __forceinline__ double sigm(double z) {
     return e / (1.0 + e);
 }
 __device__ __forceinline__ double softplus(double z) { return fmax(z, 0.0) + log1p(exp(-fabs(z))); }
+// sigma(z) (1 - sigma(z)) without cancellation
+__device__ __forceinline__ double dsig(double z) {
+    const double e = exp(-fabs(z));
+    return (e / (1.0 + e)) * (1.0 / (1.0 + e));
+}
 
-// Root s of sum_k sigma((s + u[nbr_k] - c_k)/tau) = 2 by Newton's method kept
-// inside a bracket (bisection when a step leaves it).  The bracket is the
-// smallest a_k - 40 tau (every term below 5e-18) and the third smallest
-// a_k + 40 tau (three terms above 1 - 5e-18), a_k = c_k - u[nbr_k].
-__device__ double node_root(const int32_t* nb, const float* c, int n, const double* u, double tau,
-                            double s0, int max_it) {
-    double m0 = INFINITY, m1 = INFINITY, m2 = INFINITY;
-    for (int k = 0; k < n; ++k) {
-        const double a = (double)c[k] - u[nb[k]];
-        if (a < m0) { m2 = m1; m1 = m0; m0 = a; }
-        else if (a < m1) { m2 = m1; m1 = a; }
-        else if (a < m2) { m2 = a; }
+// sum_k sigma(z_k) - 2 without cancellation: each term splits into its
+// rounding to 0 or 1 (counted exactly) and the remainder m = min(sigma,
+// 1 - sigma) = e/(1+e), e = exp(-|z|), so the tiny residuals that place a
+// root between two well-separated costs keep their relative precision.
+struct LogitAcc {
+    double cnt = 0, tail = 0, scale = 0, slope = 0;
+    __device__ __forceinline__ void add(double z) {
+        const double e = exp(-fabs(z));
+        const double m = e / (1.0 + e), big = 1.0 / (1.0 + e);
+        if (z >= 0) { cnt += 1.0; tail -= m; } else { tail += m; }
+        scale += m;
+        slope += m * big;
     }
+};
+
+// Newton's method for the root s of sum_k sigma((s - a_k)/tau) = 2 from the
+// LP root (midpoint of the 2nd and 3rd smallest a_k), kept inside the bracket
+// [smallest a_k - 40 tau, third smallest + 40 tau] by bisection; stops at a
+// relative residual of 1e-14, a step below the resolution of s or a bracket
+// of a few ulps.  `step` returns the next point, or NAN to stop.
+__device__ __forceinline__ double root_step(const LogitAcc& r, double tau, double s, double& lo,
+                                            double& hi) {
+    const double g = (r.cnt - 2.0) + r.tail, gp = r.slope / tau;
+    if (g > 0) hi = s; else lo = s;
+    if (g == 0 || fabs(g) <= 1e-14 * r.scale) return NAN;
+    double sn = (gp > 0) ? s - g / gp : 0.5 * (lo + hi);
+    if (fabs(sn - s) <= 4e-16 * (1.0 + fabs(s))) return NAN;
+    if (!(sn > lo && sn < hi)) sn = 0.5 * (lo + hi);
+    if (sn == s || hi - lo <= 4e-16 * (1.0 + fabs(s))) return NAN;
+    return sn;
+}
+
+__device__ double node_root(const int32_t* nb, const float* c, int n, const double* u, double tau,
+                            int max_it) {
+    double m0 = INFINITY, m1 = INFINITY, m2 = INFINITY;
+    for (int k = 0; k < n; ++k) top3_insert((double)c[k] - u[nb[k]], m0, m1, m2);
     double lo = m0 - 40 * tau, hi = m2 + 40 * tau;
-    double s = fmin(fmax(s0, lo), hi);
+    double s = 0.5 * (m1 + m2);
     for (int it = 0; it < max_it; ++it) {
-        double g = -2.0, gp = 0.0;
-        for (int k = 0; k < n; ++k) {
-            const double sg = sigm((s - ((double)c[k] - u[nb[k]])) / tau);
-            g += sg;
-            gp += sg * (1.0 - sg);
-        }
-        gp /= tau;
-        if (g > 0) hi = s; else lo = s;
-        if (fabs(g) <= 1e-13 || hi - lo <= 1e-15 * (1.0 + fabs(s))) break;
-        double sn = (gp > 0) ? s - g / gp : 0.5 * (lo + hi);
-        if (!(sn > lo && sn < hi)) sn = 0.5 * (lo + hi);
-        if (sn == s) break;
+        LogitAcc r;
+        for (int k = 0; k < n; ++k) r.add((s - ((double)c[k] - u[nb[k]])) / tau);
+        const double sn = root_step(r, tau, s, lo, hi);
+        if (sn != sn) break;
         s = sn;
     }
     return s;
@@ -224,7 +244,7 @@ __device__ __forceinline__ void sjacobi(const SmoothBatch& S, const SInst& I, co
                                         double* un, double* s_out) {
     for (int v = threadIdx.x; v < I.V; v += kST) {
         const int64_t a = I.row[v], e = I.row[v + 1];
-        const double s = node_root(S.nbr + a, S.c + a, (int)(e - a), u, S.tau, u[v], S.newton_max);
+        const double s = node_root(S.nbr + a, S.c + a, (int)(e - a), u, S.tau, S.newton_max);
         if (s_out) s_out[v] = s;
         un[v] = (1.0 - S.omega) * u[v] + S.omega * s;
     }
@@ -284,13 +304,13 @@ __global__ void __launch_bounds__(kST) k_sbound(SmoothBatch S) {
         double* lam = S.lam + I.base;
         double* lam2 = S.lam2 + I.base;
         for (int v = threadIdx.x; v < I.V; v += kST) {
-            double d = 2.0;
+            LogitAcc r;
             for (int64_t k = I.row[v]; k < I.row[v + 1]; ++k) {
-                const double sg = sigm((u[v] + u[S.nbr[k]] - (double)S.c[k]) / S.tau);
-                d -= sg;
-                S.gc[k] = up * (0.5 * sg);
+                const double z = (u[v] + u[S.nbr[k]] - (double)S.c[k]) / S.tau;
+                r.add(z);
+                S.gc[k] = up * (0.5 * sigm(z));
             }
-            lam[v] = up * d;
+            lam[v] = up * (-((r.cnt - 2.0) + r.tail));  // 2 - sum sigma
         }
         __syncthreads();
         double* su_ = S.segu + I.base * K;
@@ -317,8 +337,7 @@ __global__ void __launch_bounds__(kST) k_sbound(SmoothBatch S) {
                     const int64_t a = I.row[v], e = I.row[v + 1];
                     double D = 0.0;
                     for (int64_t k = a; k < e; ++k) {
-                        const double sg = sigm((st[v] + ut[S.nbr[k]] - (double)S.c[k]) / S.tau);
-                        const double p = sg * (1.0 - sg) / S.tau;
+                        const double p = dsig((st[v] + ut[S.nbr[k]] - (double)S.c[k]) / S.tau) / S.tau;
                         S.q[k] = p;
                         D += p;
                     }
@@ -361,6 +380,206 @@ __global__ void __launch_bounds__(kST) k_sbound(SmoothBatch S) {
     }
 }
 
+/* ---------------- one launch per step: a warp per node, all instances ---- */
+// The root of a node with a warp: lanes hold four a_k each in registers (the
+// first 128 list entries; later ones are re-read), top-3 and the Newton sums
+// by XOR butterflies, which give every lane the same bits, so the whole warp
+// follows one Newton path.
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+struct WNode {
+    int64_t g, base, r0;
+    int n;
+};
+__device__ __forceinline__ bool warp_node(const SmoothBatch& S, WNode& W) {
+    W.g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (W.g >= S.n_total) return false;
+    const int b = find_inst(S.offs, S.n_inst, W.g);
+    W.base = S.offs[b];
+    W.r0 = S.row[W.g];
+    W.n = (int)(S.row[W.g + 1] - W.r0);
+    return true;
+}
+
+__device__ double warp_root(const SmoothBatch& S, const WNode& W, const double* u) {
+    const int lane = threadIdx.x & 31;
+    double a[4];
+    double m0 = INFINITY, m1 = INFINITY, m2 = INFINITY;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int k = lane + 32 * j;
+        a[j] = INFINITY;
+        if (k < W.n) {
+            a[j] = (double)S.c[W.r0 + k] - u[W.base + S.nbr[W.r0 + k]];
+            top3_insert(a[j], m0, m1, m2);
+        }
+    }
+    for (int k = lane + 128; k < W.n; k += 32)
+        top3_insert((double)S.c[W.r0 + k] - u[W.base + S.nbr[W.r0 + k]], m0, m1, m2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double p0 = __shfl_xor_sync(0xffffffffu, m0, o);
+        const double p1 = __shfl_xor_sync(0xffffffffu, m1, o);
+        const double p2 = __shfl_xor_sync(0xffffffffu, m2, o);
+        top3_insert(p0, m0, m1, m2);
+        top3_insert(p1, m0, m1, m2);
+        top3_insert(p2, m0, m1, m2);
+    }
+    double lo = m0 - 40 * S.tau, hi = m2 + 40 * S.tau;
+    double s = 0.5 * (m1 + m2);
+    for (int it = 0; it < S.newton_max; ++it) {
+        LogitAcc r;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (lane + 32 * j < W.n) r.add((s - a[j]) / S.tau);
+        for (int k = lane + 128; k < W.n; k += 32)
+            r.add((s - ((double)S.c[W.r0 + k] - u[W.base + S.nbr[W.r0 + k]])) / S.tau);
+        r.cnt = warp_sum(r.cnt);
+        r.tail = warp_sum(r.tail);
+        r.scale = warp_sum(r.scale);
+        r.slope = warp_sum(r.slope);
+        const double sn = root_step(r, S.tau, s, lo, hi);
+        if (sn != sn) break;
+        s = sn;
+    }
+    return s;
+}
+
+// u -> un for every node; stores u (ust) and the roots (sst) when given, and
+// checkpoints u and the previous roots at index ck (>= 0).
+__global__ void __launch_bounds__(256) k_sw_step(SmoothBatch S, const double* u, double* un,
+                                                 double* ust, double* sst, int ck) {
+    WNode W;
+    if (!warp_node(S, W)) return;
+    if ((threadIdx.x & 31) == 0) {
+        if (ck >= 0) S.ck[(int64_t)ck * S.n_total + W.g] = u[W.g];
+        if (ust) ust[W.g] = u[W.g];
+    }
+    const double s = warp_root(S, W, u);
+    if ((threadIdx.x & 31) == 0) {
+        if (sst) sst[W.g] = s;
+        un[W.g] = (1.0 - S.omega) * u[W.g] + S.omega * s;
+    }
+}
+
+__global__ void k_sw_init(SmoothBatch S, double* u, int ck) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= S.n_total) return;
+    u[g] = ck < 0 ? 0.0 : S.ck[(int64_t)ck * S.n_total + g];
+}
+
+// per-node terms of L(u^T) and, for the adjoint, lambda^T and the explicit
+// dL/dc (sigma_e split over the edge's two slots)
+template <bool GRAD>
+__global__ void __launch_bounds__(256) k_sw_final(SmoothBatch S, const double* u) {
+    WNode W;
+    if (!warp_node(S, W)) return;
+    const int lane = threadIdx.x & 31;
+    const int b = find_inst(S.offs, S.n_inst, W.g);
+    const double up = GRAD ? S.dL[b] : 0.0;
+    const int v = (int)(W.g - W.base);
+    double sp = 0.0;
+    LogitAcc r;
+    for (int k = lane; k < W.n; k += 32) {
+        const int w = S.nbr[W.r0 + k];
+        const double z = (u[W.g] + u[W.base + w] - (double)S.c[W.r0 + k]) / S.tau;
+        if (w > v) sp += softplus(z);
+        if (GRAD) {
+            r.add(z);
+            S.gc[W.r0 + k] = up * (0.5 * sigm(z));
+        }
+    }
+    sp = warp_sum(sp);
+    if (GRAD) {
+        r.cnt = warp_sum(r.cnt);
+        r.tail = warp_sum(r.tail);
+    }
+    if (lane == 0) {
+        S.Lp[W.g] = 2.0 * u[W.g] - S.tau * sp;
+        if (GRAD) S.lam[W.g] = up * (-((r.cnt - 2.0) + r.tail));  // 2 - sum sigma
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sw_sumL(SmoothBatch S) {
+    __shared__ double sred[8];
+    const int b = blockIdx.x;
+    double x = 0.0;
+    for (int64_t g = S.offs[b] + threadIdx.x; g < S.offs[b + 1]; g += 256) x += S.Lp[g];
+    x = block_sum<256>(x, sred);
+    if (threadIdx.x == 0) S.L[b] = x;
+}
+
+__global__ void __launch_bounds__(256) k_sw_rev1(SmoothBatch S, const double* ut, const double* st,
+                                                 const double* lam) {
+    WNode W;
+    if (!warp_node(S, W)) return;
+    const int lane = threadIdx.x & 31;
+    double p[4];
+    double D = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int k = lane + 32 * j;
+        p[j] = 0.0;
+        if (k < W.n) {
+            p[j] = dsig((st[W.g] + ut[W.base + S.nbr[W.r0 + k]] - (double)S.c[W.r0 + k]) / S.tau) / S.tau;
+            D += p[j];
+        }
+    }
+    auto pk = [&](int k) {
+        return dsig((st[W.g] + ut[W.base + S.nbr[W.r0 + k]] - (double)S.c[W.r0 + k]) / S.tau) / S.tau;
+    };
+    for (int k = lane + 128; k < W.n; k += 32) D += pk(k);
+    D = warp_sum(D);
+    const double mu = D > 0 ? S.omega * lam[W.g] / D : 0.0;  // D == 0: every sigma saturated
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int k = lane + 32 * j;
+        if (k < W.n) {
+            const double q = mu * p[j];
+            S.q[W.r0 + k] = q;
+            S.gc[W.r0 + k] += q;
+        }
+    }
+    for (int k = lane + 128; k < W.n; k += 32) {
+        const double q = mu * pk(k);
+        S.q[W.r0 + k] = q;
+        S.gc[W.r0 + k] += q;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sw_rev2(SmoothBatch S, const double* lam, double* lam2) {
+    WNode W;
+    if (!warp_node(S, W)) return;
+    const int lane = threadIdx.x & 31;
+    double x = 0.0;
+    for (int k = lane; k < W.n; k += 32) x += S.q[S.mirror[W.r0 + k]];
+    x = warp_sum(x);
+    if (lane == 0) lam2[W.g] = (1.0 - S.omega) * lam[W.g] - x;
+}
+
+__global__ void k_sw_coord(SmoothBatch S) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= S.n_total) return;
+    const int b = find_inst(S.offs, S.n_inst, g);
+    const int64_t base = S.offs[b];
+    const double xv = S.x[g], yv = S.y[g];
+    double gx = 0.0, gy = 0.0;
+    for (int64_t k = S.row[g]; k < S.row[g + 1]; ++k) {
+        const double ce = (double)S.c[k];
+        if (ce == 0.0) continue;
+        const int64_t gw = base + S.nbr[k];
+        const double dc = S.gc[k] + S.gc[S.mirror[k]];
+        gx += dc * (xv - (double)S.x[gw]) / ce;
+        gy += dc * (yv - (double)S.y[gw]) / ce;
+    }
+    S.gx[g] = (float)gx;
+    S.gy[g] = (float)gy;
+}
+
 /* ---------------- host launchers ---------------------------------------- */
 static unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
@@ -381,6 +600,47 @@ cudaError_t launch_smooth_graph(SmoothBatch& S, int64_t* scan_scratch, cudaStrea
     k_scopy<<<nblk(S.n_total, 128), 128, 0, s>>>(S);
     k_smirror<<<nblk(S.n_total, 128), 128, 0, s>>>(S);
     *launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_smooth_steps(SmoothBatch& S, bool grad, cudaStream_t s, int64_t* launches) {
+    const int64_t n = S.n_total;
+    const unsigned gw = nblk(n, 8), gt = nblk(n, 256);
+    const int T = S.iters, K = S.ckpt;
+    double* u = S.ua;
+    double* un = S.ub;
+    k_sw_init<<<gt, 256, 0, s>>>(S, u, -1);
+    ++*launches;
+    for (int t = 0; t < T; ++t) {
+        k_sw_step<<<gw, 256, 0, s>>>(S, u, un, nullptr, nullptr, (grad && t % K == 0) ? t / K : -1);
+        double* tt = u; u = un; un = tt;
+    }
+    if (grad) k_sw_final<true><<<gw, 256, 0, s>>>(S, u);
+    else k_sw_final<false><<<gw, 256, 0, s>>>(S, u);
+    k_sw_sumL<<<S.n_inst, 256, 0, s>>>(S);
+    *launches += T + 2;
+    if (!grad) return cudaGetLastError();
+    double* lam = S.lam;
+    double* lam2 = S.lam2;
+    for (int seg = (T + K - 1) / K - 1; seg >= 0; --seg) {
+        const int t0 = seg * K, t1 = min(T, t0 + K);
+        u = S.ua;
+        un = S.ub;
+        k_sw_init<<<gt, 256, 0, s>>>(S, u, seg);
+        for (int t = t0; t < t1; ++t) {
+            k_sw_step<<<gw, 256, 0, s>>>(S, u, un, S.segu + (int64_t)(t - t0) * n,
+                                         S.segs + (int64_t)(t - t0) * n, -1);
+            double* tt = u; u = un; un = tt;
+        }
+        for (int t = t1 - 1; t >= t0; --t) {
+            k_sw_rev1<<<gw, 256, 0, s>>>(S, S.segu + (int64_t)(t - t0) * n, S.segs + (int64_t)(t - t0) * n, lam);
+            k_sw_rev2<<<gw, 256, 0, s>>>(S, lam, lam2);
+            double* tt = lam; lam = lam2; lam2 = tt;
+        }
+        *launches += 1 + 3 * (t1 - t0);
+    }
+    k_sw_coord<<<gt, 256, 0, s>>>(S);
+    ++*launches;
     return cudaGetLastError();
 }
 

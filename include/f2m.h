@@ -218,8 +218,10 @@ typedef struct f2m_smooth_params {
     double damping;      /* omega in (0, 1]: u <- (1-omega) u + omega root */
     int32_t newton_max;  /* Newton steps per node root */
     int32_t checkpoint;  /* steps between stored iterates in the backward pass */
+    int32_t solver;      /* 0 auto, 1 one CTA per instance, 2 one launch per step
+                            (a warp per node over the whole batch) */
 } f2m_smooth_params;
-void f2m_default_smooth_params(f2m_smooth_params* p); /* 1e-3, 100, 0.5, 60, 16 */
+void f2m_default_smooth_params(f2m_smooth_params* p); /* 1e-3, 100, 0.5, 60, 16, 0 */
 
 /* Forward: L[b] for each instance (offs has n_inst+1 entries into x/y, host
  * arrays; 3 <= top_k <= 64; at most f2m_smooth_max_nodes() points each). */

@@ -88,8 +88,35 @@ double sigmoid(double z) {
 }
 double softplus(double z) { return std::max(z, 0.0) + std::log1p(std::exp(-std::fabs(z))); }
 
-// Root s of sum_k sigma((s - a_k)/tau) = 2 (safeguarded Newton on a bracket).
-double node_root(const double* a, int n, double tau, double s0, int max_it) {
+// sum_k sigma(z_k) - 2 without cancellation: each term is split into its
+// rounding to 0 or 1 (counted exactly) and the small remainder
+// m = min(sigma, 1 - sigma) = e/(1+e), e = exp(-|z|), so the tiny residuals
+// that decide a root between two well-separated costs keep full relative
+// precision.  Also returns sum m (the scale of g) and sum sigma(1 - sigma).
+struct LogitSum {
+    double g = 0, scale = 0, slope = 0;
+};
+LogitSum logit_sum(const double* z, int n) {
+    LogitSum r;
+    int cnt = 0;
+    double tail = 0;
+    for (int k = 0; k < n; ++k) {
+        const double e = std::exp(-std::fabs(z[k]));
+        const double m = e / (1.0 + e), big = 1.0 / (1.0 + e);
+        if (z[k] >= 0) { ++cnt; tail -= m; } else { tail += m; }
+        r.scale += m;
+        r.slope += m * big;
+    }
+    r.g = (double)(cnt - 2) + tail;
+    return r;
+}
+
+// Root s of sum_k sigma((s - a_k)/tau) = 2: Newton's method from the LP root
+// (the midpoint of the 2nd and 3rd smallest a_k), kept inside a bracket by
+// bisection, stopped at a relative residual of 1e-14, a step below the
+// resolution of s, or a bracket of a few ulps.
+double node_root(const double* a, int n, double tau, int max_it) {
+    std::vector<double> z(n);
     double m0 = INFINITY, m1 = INFINITY, m2 = INFINITY;
     for (int k = 0; k < n; ++k) {
         const double v = a[k];
@@ -98,20 +125,17 @@ double node_root(const double* a, int n, double tau, double s0, int max_it) {
         else if (v < m2) { m2 = v; }
     }
     double lo = m0 - 40 * tau, hi = m2 + 40 * tau;
-    double s = std::min(std::max(s0, lo), hi);
+    double s = 0.5 * (m1 + m2);  // the LP root; exact when the costs are far apart
     for (int it = 0; it < max_it; ++it) {
-        double g = -2.0, gp = 0.0;
-        for (int k = 0; k < n; ++k) {
-            const double sg = sigmoid((s - a[k]) / tau);
-            g += sg;
-            gp += sg * (1.0 - sg);
-        }
-        gp /= tau;
+        for (int k = 0; k < n; ++k) z[k] = (s - a[k]) / tau;
+        const LogitSum r = logit_sum(z.data(), n);
+        const double g = r.g, gp = r.slope / tau;
         if (g > 0) hi = s; else lo = s;
-        if (std::fabs(g) <= 1e-13 || hi - lo <= 1e-15 * (1.0 + std::fabs(s))) break;
+        if (g == 0 || std::fabs(g) <= 1e-14 * r.scale) break;
         double sn = (gp > 0) ? s - g / gp : 0.5 * (lo + hi);
+        if (std::fabs(sn - s) <= 4e-16 * (1.0 + std::fabs(s))) break;  // step below resolution
         if (!(sn > lo && sn < hi)) sn = 0.5 * (lo + hi);
-        if (sn == s) break;
+        if (sn == s || hi - lo <= 4e-16 * (1.0 + std::fabs(s))) break;
         s = sn;
     }
     return s;
@@ -130,7 +154,7 @@ void jacobi(const SGraph& G, const std::vector<double>& u, double tau, double om
         const int64_t r0 = G.row[v], r1 = G.row[v + 1];
         a.resize(r1 - r0);
         for (int64_t k = r0; k < r1; ++k) a[k - r0] = (double)G.c[k] - u[G.nbr[k]];
-        const double s = node_root(a.data(), (int)(r1 - r0), tau, u[v], max_it);
+        const double s = node_root(a.data(), (int)(r1 - r0), tau, max_it);
         s_out[v] = s;
         un[v] = (1.0 - omega) * u[v] + omega * s;
     }
@@ -162,13 +186,14 @@ std::vector<double> backward_c(const SGraph& G, const Fwd& F, double tau, double
     std::vector<double> lam(V), lam2(V), gc(S, 0.0), q(S);
     const std::vector<double>& uT = F.u[T];
     std::vector<double> sgT(S);
+    std::vector<double> z;
     for (int v = 0; v < V; ++v) {
-        double d = 2.0;
+        z.clear();
         for (int64_t k = G.row[v]; k < G.row[v + 1]; ++k) {
-            sgT[k] = sigmoid((uT[v] + uT[G.nbr[k]] - (double)G.c[k]) / tau);
-            d -= sgT[k];
+            z.push_back((uT[v] + uT[G.nbr[k]] - (double)G.c[k]) / tau);
+            sgT[k] = sigmoid(z.back());
         }
-        lam[v] = d;
+        lam[v] = -logit_sum(z.data(), (int)z.size()).g;  // 2 - sum sigma
     }
     for (int t = T - 1; t >= 0; --t) {
         const std::vector<double>& u = F.u[t];
@@ -176,8 +201,8 @@ std::vector<double> backward_c(const SGraph& G, const Fwd& F, double tau, double
         for (int v = 0; v < V; ++v) {
             double D = 0;
             for (int64_t k = G.row[v]; k < G.row[v + 1]; ++k) {
-                const double sg = sigmoid((s[v] + u[G.nbr[k]] - (double)G.c[k]) / tau);
-                q[k] = sg * (1.0 - sg) / tau;
+                const double e = std::exp(-std::fabs((s[v] + u[G.nbr[k]] - (double)G.c[k]) / tau));
+                q[k] = (e / (1.0 + e)) * (1.0 / (1.0 + e)) / tau;
                 D += q[k];
             }
             const double mu = D > 0 ? omega * lam[v] / D : 0.0;  // D == 0: every sigma saturated

@@ -54,12 +54,13 @@ def test_oracle_cost_gradient_is_smoothed_x_at_stationarity():
 
 
 @pytest.mark.gpu
-def test_cuda_graph_and_bound_match_oracle(ctx):
+@pytest.mark.parametrize("solver", [1, 2])
+def test_cuda_graph_and_bound_match_oracle(ctx, solver):
     from oracle import oracle as O
     import f2m_b200
     x, y = synth.config4(4, 3000)
     N, iters = 30, 60
-    p = f2m_b200.default_smooth_params(tau=TAU, iters=iters)
+    p = f2m_b200.default_smooth_params(tau=TAU, iters=iters, solver=solver)
     offs = np.array([0, len(x)], np.int64)
     L, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
     Lo, dx, dy, _ = O.smooth_bound(x, y, N, tau=TAU, iters=iters, grad=True)
@@ -72,14 +73,15 @@ def test_cuda_graph_and_bound_match_oracle(ctx):
 
 
 @pytest.mark.gpu
-def test_cuda_batch_forward_adjoint_matches_oracle(ctx):
+@pytest.mark.parametrize("solver", [1, 2])
+def test_cuda_batch_forward_adjoint_matches_oracle(ctx, solver):
     """Jittered-lattice batch (the batched smoothed configuration, 24
     instances), with per-instance upstream gradients."""
     from oracle import oracle as O
     import f2m_b200
     offs, x, y = synth.config5(5, n_inst=24, lo=200, hi=600)
     N, iters = 24, 40
-    p = f2m_b200.default_smooth_params(tau=TAU, iters=iters, checkpoint=7)
+    p = f2m_b200.default_smooth_params(tau=TAU, iters=iters, checkpoint=7, solver=solver)
     up = 1.0 + np.arange(24) / 10
     L, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True, dL=up)
     for b in range(24):
