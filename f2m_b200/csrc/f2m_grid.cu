@@ -21,6 +21,33 @@ namespace f2m {
 constexpr int kGT = 512;               // threads per CTA
 constexpr long long kSpinLimit = 1LL << 26;  // ~seconds of waiting before giving up
 
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_acquire_i32(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned* p, unsigned x) {
+    unsigned v;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "r"(x) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_add_release_u32(unsigned* p, unsigned x) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(x) : "memory");
+}
+
+// Potentials written by other SMs are read through L2 (ld.global.cg): the
+// grid barrier orders the writes, and bypassing L1 keeps a stale line of an
+// earlier iteration out (the two buffers alternate every step).
+struct L2Ptr {
+    const double* p;
+    __device__ __forceinline__ double operator[](int64_t i) const { return __ldcg(p + i); }
+};
+
 struct GridSolver {
     const Batch& B;
     const DevParams& P;
@@ -39,6 +66,7 @@ struct GridSolver {
     long long* sredl;
     int* swarp;
     unsigned long long* sbcv;  // shared broadcast slot of the grid reductions
+    int* sflag;                // shared: barrier error flag of this CTA
     int phase = 0;
     long long iters = 0, wslots = 0;
     int checks = 0;
@@ -47,30 +75,34 @@ struct GridSolver {
 
     __device__ int deg(int v) const { return (int)(I.row[v + 1] - I.row[v]); }
 
-    // bounded grid barrier (count + generation)
+    // Bounded grid barrier (arrival count + generation).  Thread 0 of each CTA
+    // arrives with an acquire-release atomic (after the CTA barrier, so it
+    // releases the whole CTA's writes), the last arrival resets the count and
+    // releases the next generation, the others spin on it with acquire loads;
+    // the error flag is polled every 64 spins and broadcast through shared
+    // memory, so one thread per CTA touches the barrier words.
     __device__ bool sync() {
         __syncthreads();
-        if (threadIdx.x == 0 && *(volatile int*)G.err == 0) {
-            volatile unsigned* gen = G.bar + 1;
-            const unsigned g = *gen;
-            __threadfence();
-            const unsigned arrived = atomicAdd(G.bar, 1u);
-            if (arrived == gridDim.x - 1) {
-                G.bar[0] = 0;
-                __threadfence();
-                atomicAdd(G.bar + 1, 1u);
-            } else {
-                long long spins = 0;
-                while (*gen == g) {
-                    if (*(volatile int*)G.err != 0) break;
-                    if (++spins > kSpinLimit) { atomicExch(G.err, 1); break; }
-                    __nanosleep(64);
+        if (threadIdx.x == 0) {
+            int bad = ld_acquire_i32(G.err);
+            if (!bad) {
+                unsigned* gen = G.bar + 1;
+                const unsigned g = ld_acquire_u32(gen);
+                const unsigned arrived = atom_add_acq_rel_u32(G.bar, 1u);
+                if (arrived == gridDim.x - 1) {
+                    G.bar[0] = 0;
+                    red_add_release_u32(gen, 1u);
+                } else {
+                    for (long long spins = 1; ld_acquire_u32(gen) == g; ++spins) {
+                        if ((spins & 63) == 0 && (bad = ld_acquire_i32(G.err)) != 0) break;
+                        if (spins > kSpinLimit) { atomicExch(G.err, 1); bad = 1; break; }
+                    }
                 }
             }
-            __threadfence();
+            *sflag = bad;
         }
         __syncthreads();
-        dead = *(volatile int*)G.err != 0;
+        dead = *sflag != 0;
         return !dead;
     }
     // Deterministic grid reductions through per-CTA partials (double-buffered).
@@ -113,10 +145,12 @@ struct GridSolver {
                                   [](long long a, long long b) { return a > b ? a : b; });
     }
 
-    __device__ __forceinline__ const volatile double* hc() const { return Hc; }
+    __device__ __forceinline__ L2Ptr hc() const { return L2Ptr{Hc}; }
 
     // grad/2 of an own node over its EF list (the first efcnt slots of its
-    // list, held in shared memory or in the slot-indexed arena)
+    // list, held in shared memory or in the slot-indexed arena).  The
+    // neighbours' potentials come from L2; they are loaded four at a time
+    // ahead of the compare chain, so one L2 latency covers four entries.
     __device__ double hgrad(int v) const {
         const int n = G.efc[v];
         const int lo = sefo[v - v0];
@@ -124,23 +158,40 @@ struct GridSolver {
         const int64_t go = I.row[v] - row0;
         const double* Dp = sm ? eD + lo : G.gD + go;
         const uint32_t* Wp = sm ? eW + lo : G.gW + go;
-        const volatile double* H = hc();
+        const L2Ptr H = hc();
         const double hv = H[v];
-        auto dv = [&](int k) {
-            const uint32_t w = Wp[k];
-            const double a = H[w & 0x7fffffffu];
-            const bool first = (w >> 31) != 0;
-            return (Dp[k] + (first ? a : hv)) + (first ? hv : a);
-        };
-        double x0 = dv(0), x1 = 1e6, x2 = 1e6;
-        if (x0 < 1e6) {
-            for (int k = 1; k < n; ++k) top3_insert(dv(k), x0, x1, x2);
-        } else {
-            for (int k = 1; k < n; ++k) {
-                const double x = dv(k);
-                if (x < x0) { x2 = x1; x1 = x0; x0 = x; continue; }
-                if (x < x1) { x2 = x1; x1 = x; continue; }
-                if (x < x2) { x2 = x; }
+        constexpr int CH = 4;
+        double x0 = 0.0, x1 = 1e6, x2 = 1e6;
+        bool chain = false;
+        for (int k0 = 0; k0 < n; k0 += CH) {
+            double hw[CH], dd[CH];
+            uint32_t ww[CH];
+#pragma unroll
+            for (int j = 0; j < CH; ++j) {
+                ww[j] = 0u;
+                hw[j] = 0.0;
+                dd[j] = 0.0;
+                if (k0 + j < n) {
+                    ww[j] = Wp[k0 + j];
+                    dd[j] = Dp[k0 + j];
+                    hw[j] = H[ww[j] & 0x7fffffffu];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < CH; ++j) {
+                if (k0 + j >= n) break;
+                const bool first = (ww[j] >> 31) != 0;
+                const double x = (dd[j] + (first ? hw[j] : hv)) + (first ? hv : hw[j]);
+                if (k0 + j == 0) {  // cuda_get_Nodes_grad_R: chain unless the first is below 1e6
+                    x0 = x;
+                    chain = !(x0 < 1e6);
+                } else if (!chain) {
+                    top3_insert(x, x0, x1, x2);
+                } else {
+                    if (x < x0) { x2 = x1; x1 = x0; x0 = x; continue; }
+                    if (x < x1) { x2 = x1; x1 = x; continue; }
+                    if (x < x2) { x2 = x; }
+                }
             }
         }
         return (-(x1 + x2) / 2) * 0.5;
@@ -364,13 +415,14 @@ struct GridSolver {
     }
 };
 
-__global__ void __launch_bounds__(kGT) k_solve_grid(Batch B, DevParams P, GridState G, int b, int refit,
+__global__ void __launch_bounds__(kGT, 2) k_solve_grid(Batch B, DevParams P, GridState G, int b, int refit,
                                                      int cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sred[kGT / 32];
     __shared__ long long sredl[kGT / 32];
     __shared__ int swarp[kGT / 32 + 1];
     __shared__ unsigned long long sbc[1];
+    __shared__ int sflag[1];
     const Inst I = make_inst(B, b);
     const int V = I.V;
     const int v0 = (int)(((long long)V * blockIdx.x) / gridDim.x);
@@ -380,7 +432,7 @@ __global__ void __launch_bounds__(kGT) k_solve_grid(Batch B, DevParams P, GridSt
     const size_t head = (((size_t)nv + 1) * 4 + 15) / 16 * 16;
     double* eD = reinterpret_cast<double*>(smem_raw + head);
     uint32_t* eW = reinterpret_cast<uint32_t*>(eD + cap);
-    GridSolver S{B, P, G, I, b, v0, v1, I.row[0], G.Ha, G.Hb, eD, eW, cap, sefo, sred, sredl, swarp, sbc};
+    GridSolver S{B, P, G, I, b, v0, v1, I.row[0], G.Ha, G.Hb, eD, eW, cap, sefo, sred, sredl, swarp, sbc, sflag};
     double M;
     if (!refit) {
         for (int v = v0 + threadIdx.x; v < v1; v += kGT) G.Ha[v] = 0.0;  // F = 0
