@@ -89,7 +89,7 @@ EXPORTS = [
     "f2m_result_n_edges", "f2m_result_lp", "f2m_result_max_rank", "f2m_result_seconds",
     "f2m_result_edges", "f2m_result_nodes", "f2m_result_stats", "f2m_phase_times",
     "f2m_solve_points_noalloc", "f2m_default_smooth_params", "f2m_smoothed_bound_fwd",
-    "f2m_smoothed_bound_bwd", "f2m_smooth_max_nodes",
+    "f2m_smoothed_bound_bwd", "f2m_smooth_max_nodes", "f2m_knn",
 ]
 
 _lib = None
@@ -115,6 +115,7 @@ def lib():
         L.f2m_solve_batch.argtypes = [vp, i32, vp, vp, vp, i32, P(Params), P(BatchOut)]
         L.f2m_solve_batch_device.argtypes = [vp, i32, vp, vp, vp, vp, i32, P(Params), P(BatchOut)]
         L.f2m_solve_points.argtypes = [vp, vp, vp, vp, i32, i32, P(Params), P(vp)]
+        L.f2m_knn.argtypes = [vp, vp, vp, vp, i32, i32, P(vp)]
         L.f2m_solve_file.argtypes = [vp, ctypes.c_char_p, i32, P(Params), i32, P(vp)]
         L.f2m_result_free.argtypes = [vp]
         for name in ("f2m_result_status", "f2m_result_n_nodes", "f2m_result_n_edges",
@@ -263,6 +264,15 @@ class Context:
                                                  ctypes.byref(p), _ptr(up), _ptr(L), _ptr(gx),
                                                  _ptr(gy)))
         return L, gx, gy
+
+    def knn(self, x, y, top_k, labels=None):
+        """The kNN graph alone (edges in the reference's order; F and x are 0)."""
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        lab = None if labels is None else np.ascontiguousarray(labels, np.int32)
+        h = ctypes.c_void_p()
+        s = lib().f2m_knn(self._h, _ptr(x), _ptr(y), _ptr(lab), len(x), top_k, ctypes.byref(h))
+        return self._result(s, h)
 
     def solve_points(self, x, y, top_k, labels=None, params=None):
         x = np.ascontiguousarray(x, np.float64)

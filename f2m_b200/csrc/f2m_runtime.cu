@@ -1096,8 +1096,14 @@ f2m_status f2m_solve_batch_device(f2m_ctx* ctx, int32_t n_inst, const int64_t* h
     return F2M_OK;
 }
 
-f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels,
-                            int32_t n, int32_t top_k, const f2m_params* params, f2m_result** out) {
+}  // extern "C"
+
+namespace {
+
+// The single-instance path: rounding/de-duplication, kNN graph and, when
+// `solve`, the dual descent, comb stage and primal.
+f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels, int32_t n,
+                       int32_t top_k, const f2m_params* params, bool solve, f2m_result** out) {
     *out = nullptr;
     const int64_t offs[2] = {0, n};
     f2m_status s = check_args(ctx, 1, offs, top_k, params);
@@ -1153,6 +1159,17 @@ f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, cons
     C.B.K_in = nullptr;
     F2M_CUDA(launch_graph(C.B, C.deg, C.scan, ctx->stream, &ctx->launches));
     F2M_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+    if (!solve) {  // the graph only: edges in the reference's edge order
+        F2M_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
+        F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+        if ((s = pull_instance(ctx, C, 0, R->H, true))) return s;
+        std::fill(R->H.F.begin(), R->H.F.end(), 0.0);
+        R->status = F2M_OK;
+        R->lp = NAN;
+        R->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        *out = R.release();
+        return F2M_OK;
+    }
     if ((s = launch_classes(ctx, C, prm))) return s;
     F2M_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
     ctx->timed = true;
@@ -1174,6 +1191,20 @@ f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, cons
     R->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = R.release();
     return (f2m_status)(*out)->status;
+}
+
+}  // namespace
+
+extern "C" {
+
+f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels,
+                            int32_t n, int32_t top_k, const f2m_params* params, f2m_result** out) {
+    return points_call(ctx, x, y, labels, n, top_k, params, true, out);
+}
+
+f2m_status f2m_knn(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels, int32_t n,
+                   int32_t top_k, f2m_result** out) {
+    return points_call(ctx, x, y, labels, n, top_k, nullptr, false, out);
 }
 
 /* ------------------------------------------------------------------ */

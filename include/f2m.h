@@ -136,6 +136,14 @@ typedef struct f2m_result f2m_result;
 f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y,
                             const int32_t* labels, int32_t n, int32_t top_k,
                             const f2m_params* params, f2m_result** out);
+/* The kNN graph alone: FXY's candidate kNN (FXY.hpp:23-144, 313-534) and the
+ * greedy union of graph::graph (graph_tour.hpp:28-98), without solving.  The
+ * result carries the edges in the reference's edge order
+ * (f2m_result_edges: endpoints, labels, Do and D = Do/d_min; x is 0), the
+ * nodes (F is 0), status F2M_OK and an LP value of NaN. */
+f2m_status f2m_knn(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels,
+                   int32_t n, int32_t top_k, f2m_result** out);
+
 
 /* `F2M.solver.exe file N` (RUN.cpp:12-31): parse the TSPLIB file, solve, and
  * when write_files != 0 write <file>.topN.F2M_report / .F2M_solution

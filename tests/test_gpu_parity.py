@@ -189,3 +189,13 @@ def test_config2_100k_n50(ctx, oracle):
     r = ctx.solve_points(x, y, 50)
     _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
     assert abs(r.stats["dual_value"] - r.lp) <= 1e-9 * r.lp
+
+
+def test_knn_only_matches_oracle_graph(ctx, oracle):
+    """f2m_knn: the graph stage alone, edge for edge."""
+    x, y = synth.uniform_int_points(1500, 77)
+    o = oracle.build_graph(x, y, 14)
+    r = ctx.knn(x, y, 14)
+    assert r.status == 0 and np.isnan(r.lp)
+    assert np.array_equal(r.lab1, o.lab1) and np.array_equal(r.lab2, o.lab2)
+    assert np.array_equal(r.Do, o.Do) and np.array_equal(r.D, o.D)
