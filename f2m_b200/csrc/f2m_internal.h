@@ -41,6 +41,7 @@ struct Batch {
     int32_t N;              // neighbours selected per node (top_k, E_max)
     int32_t N_cut;          // top_k of the cut-off pass (FXY.hpp:77-78); normally N
     int32_t skip_dedup;     // points were de-duplicated on the host already
+    int32_t cost_mode;      // f2m_cost_mode of the edge costs
     int32_t n_total;        // points over all instances (before de-duplication)
     const int64_t* offs;    // [n_inst+1]
     const double* X_in;     // raw coordinates [n_total]

@@ -281,6 +281,12 @@ __device__ __forceinline__ bool key_less(double d1, int e1, int o1, double d2, i
 // lanes (position lane*RPL + r); candidates come from the cells within the
 // node's cut-off radius, which holds all of its first N (their distances are
 // below the cut-off, FXY.hpp:486-502).  Insertion is a warp-wide shift.
+// Edge cost of a candidate at FP64 distance d: the reference's raw distance,
+// or TSPLIB EUC_2D nint(d) (the oracle's ORC_COST_NINT).
+__device__ __forceinline__ double cand_cost(double d, int mode) {
+    return mode == F2M_COST_NINT ? (double)(long long)(d + 0.5) : d;
+}
+
 template <int RPL>
 __global__ void __launch_bounds__(kT) k_select(Batch B) {
     const int c = blockIdx.x;
@@ -293,74 +299,111 @@ __global__ void __launch_bounds__(kT) k_select(Batch B) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int N = min(B.N, V - 1);
     const int nx = B.gnx[b];
+    const int mode = B.cost_mode;
     const unsigned FULL = 0xffffffffu;
     for (int qi = w; qi < kT && i0 + qi < V; qi += kT / 32) {
         const int i = i0 + qi;
         const double2 me = B.P[base + i];
-        const double R = B.cut[base + i];
+        const double cut_i = B.cut[base + i];
         double kd[RPL];
         int ke[RPL], ko[RPL];
 #pragma unroll
         for (int r = 0; r < RPL; ++r) { kd[r] = INFINITY; ke[r] = INT_MAX; ko[r] = INT_MAX; }
         int cnt = 0;
         double worst_hi = INFINITY;
-        const Box bx = box_of(B, b, me.x, me.y, R);
-        for (int cy = bx.cy0; cy <= bx.cy1; ++cy) {
-            const int64_t k0 = B.cellstart[base + cy * nx + bx.cx0];
-            const int64_t k1 = B.cellstart[base + cy * nx + bx.cx1 + 1];
-            for (int64_t kb = k0; kb < k1; kb += 32) {
-                const int64_t k = kb + lane;
-                bool pass = false;
-                double d = 0.0;
-                int em = 0, oth = 0;
-                if (k < k1) {
-                    const int j = B.sidx[k];
-                    const double2 p = B.spt[k];
-                    const double dX = fabs(me.x - p.x), dY = fabs(me.y - p.y);
-                    const double q = fma(dY, dY, dX * dX);
-                    if (j != i && (cnt < N || q <= worst_hi)) {
-                        pass = true;
-                        d = sqrt(q);
-                        em = i;
-                        oth = j;
-                        if (j < i && d <= B.cut[base + j]) { em = j; oth = i; }
+        // Pass 0 scans the cells around the node's own cut-off radius, where its
+        // first N candidates lie.  With nint costs a candidate out to
+        // (N-th cost + 0.5) can tie with the N-th, so pass 1 scans the cells of
+        // that wider box that pass 0 did not.
+        Box bx0 = box_of(B, b, me.x, me.y, cut_i);
+        for (int pass = 0; pass < 2; ++pass) {
+            Box bx = bx0;
+            if (pass == 1) {
+                if (mode != F2M_COST_NINT || cnt < N) break;
+                const int wl = (N - 1) / RPL, wr = (N - 1) % RPL;
+                double mineD = 0.0;
+#pragma unroll
+                for (int r = 0; r < RPL; ++r)
+                    if (r == wr) mineD = kd[r];
+                const double R2 = __shfl_sync(FULL, mineD, wl) + 0.5;
+                if (!(R2 > cut_i)) break;
+                bx = box_of(B, b, me.x, me.y, R2);
+            }
+            for (int cy = bx.cy0; cy <= bx.cy1; ++cy) {
+                for (int cx0 = bx.cx0; cx0 <= bx.cx1;) {
+                    // a run of cells on this row (pass 1: outside pass 0's box)
+                    int cx1 = bx.cx1;
+                    if (pass == 1 && cy >= bx0.cy0 && cy <= bx0.cy1) {
+                        if (cx0 >= bx0.cx0 && cx0 <= bx0.cx1) { cx0 = bx0.cx1 + 1; continue; }
+                        if (cx0 < bx0.cx0) cx1 = min(cx1, bx0.cx0 - 1);
                     }
-                }
-                unsigned mask = __ballot_sync(FULL, pass);
-                while (mask) {
-                    const int src = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const double cd = __shfl_sync(FULL, d, src);
-                    const int ce = __shfl_sync(FULL, em, src);
-                    const int co = __shfl_sync(FULL, oth, src);
-                    int mine = 0;
-#pragma unroll
-                    for (int r = 0; r < RPL; ++r)
-                        if (lane * RPL + r < cnt && key_less(kd[r], ke[r], ko[r], cd, ce, co)) mine++;
-                    const int pos = (int)__reduce_add_sync(FULL, mine);
-                    if (pos >= N) continue;
-                    const double pd = __shfl_up_sync(FULL, kd[RPL - 1], 1);
-                    const int pe = __shfl_up_sync(FULL, ke[RPL - 1], 1);
-                    const int po = __shfl_up_sync(FULL, ko[RPL - 1], 1);
-#pragma unroll
-                    for (int r = RPL - 1; r >= 0; --r) {
-                        const int g = lane * RPL + r;
-                        if (g > pos) {
-                            if (r > 0) { kd[r] = kd[r - 1]; ke[r] = ke[r - 1]; ko[r] = ko[r - 1]; }
-                            else { kd[r] = pd; ke[r] = pe; ko[r] = po; }
-                        } else if (g == pos) {
-                            kd[r] = cd; ke[r] = ce; ko[r] = co;
+                    const int64_t k0 = B.cellstart[base + cy * nx + cx0];
+                    const int64_t k1 = B.cellstart[base + cy * nx + cx1 + 1];
+                    cx0 = cx1 + 1;
+                    for (int64_t kb = k0; kb < k1; kb += 32) {
+                        const int64_t k = kb + lane;
+                        bool take = false;
+                        double cd_ = 0.0;
+                        int em = 0, oth = 0;
+                        if (k < k1) {
+                            const int j = B.sidx[k];
+                            const double2 p = B.spt[k];
+                            const double dX = fabs(me.x - p.x), dY = fabs(me.y - p.y);
+                            const double q = fma(dY, dY, dX * dX);
+                            if (j != i && (cnt < N || q <= worst_hi)) {
+                                const double d = sqrt(q);
+                                const double cut_j = B.cut[base + j];
+                                // a candidate of the reference (FXY.hpp:388-432):
+                                // within either endpoint's cut-off; the lower id
+                                // emits it if within its own cut-off
+                                take = d <= cut_i || d <= cut_j;
+                                const int a = min(i, j), bb = max(i, j);
+                                const double cut_a = (a == i) ? cut_i : cut_j;
+                                em = (d <= cut_a) ? a : bb;
+                                oth = (em == a) ? bb : a;
+                                cd_ = cand_cost(d, mode);
+                            }
                         }
-                    }
-                    cnt = min(cnt + 1, N);
-                    if (cnt == N) {
-                        const int wl = (N - 1) / RPL, wr = (N - 1) % RPL;
-                        double mineD = 0.0;
+                        unsigned mask = __ballot_sync(FULL, take);
+                        while (mask) {
+                            const int src = __ffs(mask) - 1;
+                            mask &= mask - 1;
+                            const double cd = __shfl_sync(FULL, cd_, src);
+                            const int ce = __shfl_sync(FULL, em, src);
+                            const int co = __shfl_sync(FULL, oth, src);
+                            int mine = 0;
 #pragma unroll
-                        for (int r = 0; r < RPL; ++r)
-                            if (r == wr) mineD = kd[r];
-                        const double wd = __shfl_sync(FULL, mineD, wl);
-                        worst_hi = wd * wd * (1.0 + 0x1p-40);
+                            for (int r = 0; r < RPL; ++r)
+                                if (lane * RPL + r < cnt && key_less(kd[r], ke[r], ko[r], cd, ce, co)) mine++;
+                            const int pos = (int)__reduce_add_sync(FULL, mine);
+                            if (pos >= N) continue;
+                            const double pd = __shfl_up_sync(FULL, kd[RPL - 1], 1);
+                            const int pe = __shfl_up_sync(FULL, ke[RPL - 1], 1);
+                            const int po = __shfl_up_sync(FULL, ko[RPL - 1], 1);
+#pragma unroll
+                            for (int r = RPL - 1; r >= 0; --r) {
+                                const int g = lane * RPL + r;
+                                if (g > pos) {
+                                    if (r > 0) { kd[r] = kd[r - 1]; ke[r] = ke[r - 1]; ko[r] = ko[r - 1]; }
+                                    else { kd[r] = pd; ke[r] = pe; ko[r] = po; }
+                                } else if (g == pos) {
+                                    kd[r] = cd; ke[r] = ce; ko[r] = co;
+                                }
+                            }
+                            cnt = min(cnt + 1, N);
+                            if (cnt == N) {
+                                const int wl = (N - 1) / RPL, wr = (N - 1) % RPL;
+                                double mineD = 0.0;
+#pragma unroll
+                                for (int r = 0; r < RPL; ++r)
+                                    if (r == wr) mineD = kd[r];
+                                const double wd = __shfl_sync(FULL, mineD, wl);
+                                // squared-distance bound of a key that can still
+                                // enter (raw: <= wd; nint: < wd + 0.5)
+                                const double wr_ = (mode == F2M_COST_NINT) ? wd + 0.5 : wd;
+                                worst_hi = wr_ * wr_ * (1.0 + 0x1p-40);
+                            }
+                        }
                     }
                 }
             }
@@ -407,7 +450,11 @@ __global__ void __launch_bounds__(kT) k_graph_rev(Batch B) {
     }
     // d_min over kept edges (graph_tour.hpp:70): the smallest cost of a
     // node's list is its first entry; positive doubles order like their bits
-    if (nt > 0) atomicMin(&B.dmin_bits[b], (unsigned long long)__double_as_longlong(B.top_cost[o]));
+    if (nt > 0) {
+        atomicMin(&B.dmin_bits[b], (unsigned long long)__double_as_longlong(B.top_cost[o]));
+        // a zero-cost edge (nint of a distance below 0.5) leaves D undefined
+        if (B.top_cost[o] == 0.0) B.status[b] = F2M_ERR_INPUT;
+    }
 }
 
 // degree per input position (0 for dropped duplicates and padding)

@@ -597,6 +597,7 @@ f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h
     carve(A, C.B, C.pl, own_inputs, &C.deg, &C.scan, &C.ci, &C.cs, &C.ord);
     if (C.grid) carve_grid(A, C.G, std::max<int64_t>(C.pl.n_total, 1), C.B.S_cap);
     C.B.skip_dedup = 0;
+    C.B.cost_mode = prm.cost_mode;
     // work lists through pinned staging
     const size_t nc = C.pl.chunk_inst.size();
     const size_t bytes = (2 * nc + n_inst) * sizeof(int32_t);
@@ -967,8 +968,8 @@ static f2m_status check_args(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, 
     if (n_inst < 1 || !offs) return fail(ctx, F2M_ERR_INPUT, "need at least one instance");
     if (top_k < 3) return fail(ctx, F2M_ERR_INPUT, "N must be at least 3");
     if (top_k > 256) return fail(ctx, F2M_ERR_CAPACITY, "N above 256 is not supported");
-    if (params && params->cost_mode != F2M_COST_REF_EUCLID)
-        return fail(ctx, F2M_ERR_INPUT, "only the reference cost mode runs on the device");
+    if (params && params->cost_mode != F2M_COST_REF_EUCLID && params->cost_mode != F2M_COST_NINT)
+        return fail(ctx, F2M_ERR_INPUT, "unknown cost mode");
     for (int32_t b = 0; b < n_inst; ++b)
         if (offs[b + 1] < offs[b]) return fail(ctx, F2M_ERR_INPUT, "offsets must be non-decreasing");
     if (offs[0] != 0) return fail(ctx, F2M_ERR_INPUT, "offs[0] must be 0");

@@ -28,7 +28,7 @@ typedef enum f2m_status {
 
 typedef enum f2m_cost_mode {
     F2M_COST_REF_EUCLID = 0,    /* raw FP64 sqrt(dx^2+dy^2), as FXY.hpp:382 */
-    F2M_COST_NINT = 1           /* TSPLIB EUC_2D nint(); oracle-only for now */
+    F2M_COST_NINT = 1           /* TSPLIB EUC_2D nint(sqrt(dx^2+dy^2)) as the edge cost */
 } f2m_cost_mode;
 
 /* The reference's hard-coded constants, now parameters (defaults equal the

@@ -199,3 +199,31 @@ def test_knn_only_matches_oracle_graph(ctx, oracle):
     assert r.status == 0 and np.isnan(r.lp)
     assert np.array_equal(r.lab1, o.lab1) and np.array_equal(r.lab2, o.lab2)
     assert np.array_equal(r.Do, o.Do) and np.array_equal(r.D, o.D)
+
+
+# --- TSPLIB EUC_2D costs: nint(distance) as the edge cost --------------------
+
+def test_nint_cost_mode_matches_oracle(ctx, oracle):
+    """Integer costs tie often: the nint key order and the widened candidate
+    search (ties with the N-th cost out to cost + 0.5)."""
+    p = f2m_b200.default_params(cost_mode=1)
+    for seed, n, N in [(51, 1000, 20), (52, 400, 8), (53, 2500, 16)]:
+        x, y = synth.uniform_int_points(n, seed)
+        o = oracle.solve_points(x, y, N, cost=oracle.COST_NINT)
+        r = ctx.solve_points(x, y, N, params=p)
+        _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+    x, y = synth.lattice_points(300, 5)
+    o = oracle.solve_points(x, y, 8, cost=oracle.COST_NINT)
+    r = ctx.solve_points(x, y, 8, params=p)
+    _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
+
+
+def test_nint_batch_matches_oracle(ctx, oracle):
+    offs, x, y = synth.config3(seed=8, n_inst=30, hi=1200)
+    p = f2m_b200.default_params(cost_mode=1)
+    lp, st = ctx.solve_batch(offs, x, y, 16, params=p)
+    lp_o, st_o, _ = oracle.solve_batch(offs, x, y, 16, cost=oracle.COST_NINT,
+                                       threads=os.cpu_count() or 1)
+    assert np.array_equal(st, st_o)
+    ok = st_o == 0
+    assert np.all(np.abs(lp[ok] - lp_o[ok]) <= LP_RTOL * np.abs(lp_o[ok]))
