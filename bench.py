@@ -250,6 +250,7 @@ def ours_arm(args, rank, world, local_rank):
     import f2m_b200
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    tuned = f2m_b200.load_tuning()  # size-class bounds from f2m_b200/autotune.py
     offs, x, y = workload(rank, args.n_inst, args.size_range)
     n_inst = len(offs) - 1
     ctx = f2m_b200.Context(local_rank)
@@ -374,6 +375,7 @@ def ours_arm(args, rank, world, local_rank):
                        "one f2m_solve_batch_device call each", "speedup": value / world / plain,
                        "max_lp_rel_err_vs_batched": plain_err},
         "iterations_mean": float(work["node_iters"] / max(work["points"], 1)),
+        "class_bounds": f2m_b200.get_class_bounds(), "class_bounds_tuned": tuned is not None,
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(offs, x, y)

@@ -89,7 +89,8 @@ EXPORTS = [
     "f2m_result_n_edges", "f2m_result_lp", "f2m_result_max_rank", "f2m_result_seconds",
     "f2m_result_edges", "f2m_result_nodes", "f2m_result_stats", "f2m_phase_times",
     "f2m_solve_points_noalloc", "f2m_default_smooth_params", "f2m_smoothed_bound_fwd",
-    "f2m_smoothed_bound_bwd", "f2m_smooth_max_nodes", "f2m_knn",
+    "f2m_smoothed_bound_bwd", "f2m_smooth_max_nodes", "f2m_knn", "f2m_set_class_bounds",
+    "f2m_get_class_bounds",
 ]
 
 _lib = None
@@ -135,6 +136,8 @@ def lib():
         L.f2m_smoothed_bound_bwd.argtypes = [vp, i32, vp, vp, vp, i32, P(SmoothParams), vp, vp,
                                              vp, vp]
         L.f2m_smooth_max_nodes.restype = i32
+        L.f2m_set_class_bounds.argtypes = [vp]
+        L.f2m_get_class_bounds.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -145,6 +148,32 @@ def default_params(**overrides):
     for k, v in overrides.items():
         setattr(p, k, v)
     return p
+
+
+def set_class_bounds(bounds):
+    """Size-class bounds of the batched solver (3 increasing point counts)."""
+    b = np.ascontiguousarray(bounds, np.int32)
+    s = lib().f2m_set_class_bounds(b.ctypes.data_as(ctypes.c_void_p))
+    if s != OK:
+        raise F2MError(s, f"class bounds {list(bounds)} rejected")
+
+
+def get_class_bounds():
+    b = np.zeros(3, np.int32)
+    lib().f2m_get_class_bounds(b.ctypes.data_as(ctypes.c_void_p))
+    return [int(v) for v in b]
+
+
+def load_tuning(path=None):
+    """Apply the class bounds recorded by f2m_b200.autotune (default: the
+    committed f2m_b200/tuned_classes.json); returns them, or None."""
+    import json
+    path = path or os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_classes.json")
+    if not os.path.exists(path):
+        return None
+    bounds = json.load(open(path))["bounds"]
+    set_class_bounds(bounds)
+    return bounds
 
 
 def default_smooth_params(**overrides):

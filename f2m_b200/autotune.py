@@ -1,0 +1,103 @@
+"""Autotuner for the size classes of the batched solver.
+
+The batched solver runs each instance on a team of 128, 256, 512 or 1024
+threads (8, 4, 2 or 1 teams per CTA) chosen by its point count; the three
+bounds between the classes decide how shared memory and SMs are split
+across a batch of uneven instances.  The potentials never depend on them
+(the LP value only through the order of a sum).  This script times the
+solve phase (CUDA events) of a workload under a grid of candidate bounds,
+re-times the five fastest with more repetitions, and records the one with
+the lowest median in a JSON file that `f2m_b200.load_tuning()` applies:
+
+    python -m f2m_b200.autotune                    # 4,096-instance synthetic batch
+    python -m f2m_b200.autotune --out my_tuning.json --n-inst 1024 --hi 3000
+"""
+import argparse
+import itertools
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_OUT = os.path.join(HERE, "tuned_classes.json")
+
+GRID = {
+    "a": (320, 448, 576),
+    "b": (768, 896, 1152, 1408),
+    "c": (1536, 1792, 2304, 2816, 3328),
+}
+
+
+def time_bounds(ctx, offs, x, y, top_k, bounds, reps):
+    """Median solve-phase ms over `reps` calls after one warm-up call."""
+    import f2m_b200
+    f2m_b200.set_class_bounds(bounds)
+    ctx.solve_batch(offs, x, y, top_k)  # warm-up (and arena growth)
+    t = []
+    for _ in range(reps):
+        ctx.solve_batch(offs, x, y, top_k)
+        ms, _ = ctx.phase_times()
+        t.append(float(ms[3]))
+    return float(np.median(t))
+
+
+def autotune(offs, x, y, top_k, reps=2, grid=GRID, ctx=None, log=None, final_reps=5, finalists=5):
+    """Time every increasing combination of the grid, then the fastest few
+    again; returns (best bounds, its median solve ms, table of (bounds, ms))."""
+    import f2m_b200
+    own = ctx is None
+    ctx = ctx or f2m_b200.Context(0)
+    start = f2m_b200.get_class_bounds()
+    table = []
+    try:
+        for a, b, c in itertools.product(grid["a"], grid["b"], grid["c"]):
+            if not a < b < c:
+                continue
+            try:
+                ms = time_bounds(ctx, offs, x, y, top_k, [a, b, c], reps)
+            except f2m_b200.F2MError:
+                continue  # a class cannot hold instances that large
+            table.append(([a, b, c], ms))
+            if log:
+                log(f"bounds {a:5d} {b:5d} {c:5d}: solve {ms:8.2f} ms")
+        final = []
+        for bounds, _ in sorted(table, key=lambda t: t[1])[:finalists]:
+            ms = time_bounds(ctx, offs, x, y, top_k, bounds, final_reps)
+            final.append((bounds, ms))
+            if log:
+                log(f"final  {bounds}: solve {ms:8.2f} ms (median of {final_reps})")
+    finally:
+        f2m_b200.set_class_bounds(start)
+        if own:
+            ctx.close()
+    bounds, ms = min(final, key=lambda t: t[1])
+    return bounds, ms, table
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--n-inst", type=int, default=4096)
+    ap.add_argument("--lo", type=int, default=50)
+    ap.add_argument("--hi", type=int, default=5000)
+    ap.add_argument("--top-k", type=int, default=16)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--reps", type=int, default=2)
+    args = ap.parse_args(argv)
+    sys.path.insert(0, os.path.dirname(HERE))
+    from f2m_b200 import synth
+    offs, x, y = synth.config3(seed=args.seed, n_inst=args.n_inst, lo=args.lo, hi=args.hi)
+    bounds, ms, table = autotune(offs, x, y, args.top_k, reps=args.reps, log=print)
+    rec = {"bounds": bounds, "solve_ms": ms,
+           "workload": {"n_inst": args.n_inst, "sizes": "log-uniform", "lo": args.lo, "hi": args.hi,
+                        "top_k": args.top_k, "seed": args.seed},
+           "table": [{"bounds": b, "solve_ms": t} for b, t in table]}
+    with open(args.out, "w") as f:
+        json.dump(rec, f, indent=1)
+    print(f"best bounds {bounds}: solve {ms:.2f} ms -> {args.out}")
+
+
+if __name__ == "__main__":
+    main()

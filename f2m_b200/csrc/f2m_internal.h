@@ -154,6 +154,8 @@ cudaError_t launch_refit_class(int c, const Batch& B, const DevParams& P, const 
                                int64_t* launches);
 int solve_num_classes();
 int solve_class_of(int32_t n);
+int solve_set_bounds(const int32_t* max_n);  // 3 increasing bounds; -1 if rejected
+void solve_get_bounds(int32_t* max_n);
 // Smoothed-bound batch (f2m_smooth.cu).  Node g of instance b is offs[b] +
 // local id; neighbour ids in nbr are local; slots are global (row).
 struct SmoothBatch {

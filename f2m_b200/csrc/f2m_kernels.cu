@@ -1292,9 +1292,28 @@ cudaError_t launch_graph(const Batch& B, int64_t* deg, int64_t* scan_scratch, cu
 struct SolveClass {
     int team, teams, max_n;
 };
-static const SolveClass kClasses[] = {
+// Size classes: instances of at most max_n points go to the first class that
+// takes them.  The bounds are tunable per process (solve_set_bounds); the
+// defaults came from timing the batched workload on a B200.
+static SolveClass kClasses[] = {
     {128, 8, 448}, {256, 4, 896}, {512, 2, 1792}, {1024, 1, 1 << 30}};
 constexpr int kNumClasses = 4;
+
+// Largest instance whose fixed shared-memory part fits a team of class c.
+static int class_capacity(int c);
+
+int solve_set_bounds(const int32_t* max_n) {
+    int prev = 3;
+    for (int c = 0; c < kNumClasses - 1; ++c) {
+        if (max_n[c] <= prev || max_n[c] > class_capacity(c)) return -1;
+        prev = max_n[c];
+    }
+    for (int c = 0; c < kNumClasses - 1; ++c) kClasses[c].max_n = max_n[c];
+    return 0;
+}
+void solve_get_bounds(int32_t* max_n) {
+    for (int c = 0; c < kNumClasses - 1; ++c) max_n[c] = kClasses[c].max_n;
+}
 
 int32_t solve_max_nodes() { return 10000; }
 int solve_num_classes() { return kNumClasses; }
@@ -1311,12 +1330,27 @@ static size_t smem_per_block() {
     return (size_t)v;
 }
 
+static int team_bytes_of(int team, int teams) {
+    const size_t stat = sizeof(double) * teams * (team / 32) * 2 + sizeof(int) * teams * (team / 32 + 5) + 64;
+    const size_t dyn = (smem_per_block() - stat) & ~(size_t)255;
+    return (int)((dyn / teams) & ~(size_t)15);
+}
+static int class_capacity(int c) {
+    const int tb = team_bytes_of(kClasses[c].team, kClasses[c].teams);
+    int lo = 4, hi = 32767;  // node ids are 15-bit in the EF words
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (team_fixed_bytes(mid) <= (size_t)tb) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 template <int TEAM, int TEAMS, bool R>
 static cudaError_t launch_one(const Batch& B, const DevParams& P, const int32_t* items, int n_items,
                               int32_t* queue, int vcap, cudaStream_t s, int64_t* launches) {
     const size_t stat = sizeof(double) * TEAMS * (TEAM / 32) * 2 + sizeof(int) * TEAMS * (TEAM / 32 + 5) + 64;
     const size_t dyn = (smem_per_block() - stat) & ~(size_t)255;
-    const int team_bytes = (int)((dyn / TEAMS) & ~(size_t)15);
+    const int team_bytes = team_bytes_of(TEAM, TEAMS);
     if (team_fixed_bytes(vcap) > (size_t)team_bytes) return cudaErrorInvalidConfiguration;
     cudaError_t e = cudaFuncSetAttribute(k_solve<TEAM, TEAMS, R>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);

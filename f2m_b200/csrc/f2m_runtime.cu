@@ -1222,6 +1222,12 @@ void f2m_default_smooth_params(f2m_smooth_params* p) {
 
 int32_t f2m_smooth_max_nodes(void) { return smooth_max_nodes(); }
 
+f2m_status f2m_set_class_bounds(const int32_t* max_nodes) {
+    if (!max_nodes) return F2M_ERR_INPUT;
+    return solve_set_bounds(max_nodes) == 0 ? F2M_OK : F2M_ERR_INPUT;
+}
+void f2m_get_class_bounds(int32_t* max_nodes) { solve_get_bounds(max_nodes); }
+
 }  // extern "C"
 
 namespace {

@@ -244,6 +244,17 @@ f2m_status f2m_smoothed_bound_bwd(f2m_ctx* ctx, int32_t n_inst, const int64_t* o
                                   float* dL_dx, float* dL_dy);
 int32_t f2m_smooth_max_nodes(void);
 
+/* Size classes of the batched solver (no reference counterpart): an instance
+ * of at most max_nodes[0] points runs on a 128-thread team (8 per CTA), up to
+ * max_nodes[1] on 256 (4 per CTA), up to max_nodes[2] on 512 (2 per CTA),
+ * larger ones on 1024 threads.  The potentials do not depend on the classes
+ * (the LP value only through the order of its team-wide sum, ~1e-16
+ * relative); f2m_b200/autotune.py times candidate bounds on a workload.  The
+ * bounds are process-wide: set them before solving.  F2M_ERR_INPUT if not
+ * increasing or a class's shared memory cannot hold an instance that size. */
+f2m_status f2m_set_class_bounds(const int32_t* max_nodes); /* 3 values */
+void f2m_get_class_bounds(int32_t* max_nodes);
+
 #ifdef __cplusplus
 }
 #endif

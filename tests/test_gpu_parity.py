@@ -227,3 +227,21 @@ def test_nint_batch_matches_oracle(ctx, oracle):
     assert np.array_equal(st, st_o)
     ok = st_o == 0
     assert np.all(np.abs(lp[ok] - lp_o[ok]) <= LP_RTOL * np.abs(lp_o[ok]))
+
+
+def test_class_bounds_change_speed_not_results(ctx):
+    """The size classes only decide which team size runs an instance."""
+    offs, x, y = synth.config3(seed=12, n_inst=24, hi=2500)
+    start = f2m_b200.get_class_bounds()
+    lp0, st0 = ctx.solve_batch(offs, x, y, 16)
+    try:
+        f2m_b200.set_class_bounds([100, 200, 300])
+        lp1, st1 = ctx.solve_batch(offs, x, y, 16)
+        with pytest.raises(f2m_b200.F2MError):
+            f2m_b200.set_class_bounds([500, 400, 900])
+    finally:
+        f2m_b200.set_class_bounds(start)
+    # the potentials are the same bits; the LP value is a team-wide sum whose
+    # order follows the team size
+    assert np.array_equal(st0, st1)
+    assert np.all(np.abs(lp0 - lp1) <= LP_RTOL * np.abs(lp0))
