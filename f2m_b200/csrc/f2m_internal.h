@@ -78,6 +78,7 @@ struct Batch {
     // graph
     int32_t* rev;           // [n_total]
     int32_t* cursor;        // [n_total]
+    uint8_t* tdup;          // [n_total * N] the top entry's neighbour also keeps this node
     int64_t* row;           // [n_total+1]
     int32_t* s_nbr;         // [S]
     double* s_cost;         // [S] raw cost Do

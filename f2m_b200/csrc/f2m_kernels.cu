@@ -446,7 +446,9 @@ __global__ void __launch_bounds__(kT) k_graph_rev(Batch B) {
     const int nt = B.ntop[base + i];
     for (int k = 0; k < nt; ++k) {
         const int j = B.top_nbr[o + k];
-        if (!in_top(B, base, j, i)) atomicAdd(&B.rev[base + j], 1);
+        const bool dup = in_top(B, base, j, i);
+        B.tdup[o + k] = dup;
+        if (!dup) atomicAdd(&B.rev[base + j], 1);
     }
     // d_min over kept edges (graph_tour.hpp:70): the smallest cost of a
     // node's list is its first entry; positive doubles order like their bits
@@ -486,7 +488,7 @@ __global__ void __launch_bounds__(kT) k_graph_fill(Batch B) {
         const double cost = B.top_cost[o + k];
         const int em = B.top_em[o + k], oth = B.top_oth[o + k];
         B.s_nbr[r + k] = j; B.s_cost[r + k] = cost; B.s_em[r + k] = em; B.s_oth[r + k] = oth;
-        if (!in_top(B, base, j, i)) {
+        if (!B.tdup[o + k]) {
             const int p = atomicAdd(&B.cursor[base + j], 1);
             const int64_t s2 = B.row[base + j] + B.ntop[base + j] + p;
             B.s_nbr[s2] = i; B.s_cost[s2] = cost; B.s_em[s2] = em; B.s_oth[s2] = oth;
@@ -506,6 +508,26 @@ __global__ void __launch_bounds__(kT) k_graph_sort(Batch B) {
     const int64_t base = B.offs[b];
     const int64_t r0 = B.row[base + i], r1 = B.row[base + i + 1];
     if (r1 - r0 > 65535) { B.status[b] = F2M_ERR_CAPACITY; return; }
+    constexpr int kLocal = 48;  // lists up to this long are sorted in registers/local memory
+    const int n = (int)(r1 - r0);
+    if (n <= kLocal) {
+        double kd[kLocal];
+        int ke[kLocal], ko[kLocal], kn[kLocal];
+        for (int a = 0; a < n; ++a) {
+            const double d = B.s_cost[r0 + a];
+            const int e = B.s_em[r0 + a], o2 = B.s_oth[r0 + a], nb = B.s_nbr[r0 + a];
+            int p = a;
+            while (p > 0 && key_less(d, e, o2, kd[p - 1], ke[p - 1], ko[p - 1])) {
+                kd[p] = kd[p - 1]; ke[p] = ke[p - 1]; ko[p] = ko[p - 1]; kn[p] = kn[p - 1];
+                --p;
+            }
+            kd[p] = d; ke[p] = e; ko[p] = o2; kn[p] = nb;
+        }
+        for (int a = 0; a < n; ++a) {
+            B.s_cost[r0 + a] = kd[a]; B.s_em[r0 + a] = ke[a];
+            B.s_oth[r0 + a] = ko[a]; B.s_nbr[r0 + a] = kn[a];
+        }
+    } else {
     for (int64_t a = r0 + 1; a < r1; ++a) {
         const double kd = B.s_cost[a];
         const int ke = B.s_em[a], ko = B.s_oth[a], kn = B.s_nbr[a];
@@ -516,6 +538,7 @@ __global__ void __launch_bounds__(kT) k_graph_sort(Batch B) {
             --p;
         }
         B.s_cost[p] = kd; B.s_em[p] = ke; B.s_oth[p] = ko; B.s_nbr[p] = kn;
+    }
     }
     const double dmin = __longlong_as_double((long long)B.dmin_bits[b]);
     for (int64_t a = r0; a < r1; ++a) {
@@ -538,12 +561,18 @@ __global__ void __launch_bounds__(kT) k_graph_mirror(Batch B) {
     const int64_t base = B.offs[b];
     const int64_t r0 = B.row[base + i], r1 = B.row[base + i + 1];
     for (int64_t a = r0; a < r1; ++a) {
+        // the same edge carries the same key in both lists, and both lists
+        // are sorted by key: binary search
         const int j = B.s_nbr[a];
-        const int64_t q0 = B.row[base + j], q1 = B.row[base + j + 1];
-        int m = -1;
-        for (int64_t q = q0; q < q1; ++q)
-            if (B.s_nbr[q] == i) { m = (int)(q - q0); break; }
-        B.mirror[a] = m;
+        const double kd = B.s_cost[a];
+        const int ke = B.s_em[a], ko = B.s_oth[a];
+        int64_t lo = B.row[base + j], hi = B.row[base + j + 1];
+        const int64_t q0 = lo;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (key_less(B.s_cost[mid], B.s_em[mid], B.s_oth[mid], kd, ke, ko)) lo = mid + 1; else hi = mid;
+        }
+        B.mirror[a] = (lo < B.row[base + j + 1] && B.s_nbr[lo] == i) ? (int)(lo - q0) : -1;
     }
 }
 

@@ -242,6 +242,7 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.top_oth = A.take<int32_t>(nN);
     B.rev = A.take<int32_t>(n);
     B.cursor = A.take<int32_t>(n);
+    B.tdup = A.take<uint8_t>(nN);
     B.row = A.take<int64_t>(n + 1);
     B.s_nbr = A.take<int32_t>(S);
     B.s_cost = A.take<double>(S);
