@@ -980,8 +980,10 @@ static f2m_status check_args(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, 
 
 // Host completion of the batch instances whose combs need the Ax=b stage.
 // Instances whose combs need the host stage (comb_thread.cpp, Ax_b.cpp) are
-// completed by a pool of host threads; copies and repair refits on the GPU
-// are serialised by a mutex, the host comb checks run side by side.
+// completed by a pool of host threads.  Their device state is first copied
+// in one go into pinned staging (one synchronisation for all of them); the
+// threads then rebuild the host instances and run the comb checks side by
+// side, and any repair refits share the call's stream under a mutex.
 static f2m_status complete_batch(f2m_ctx* ctx, DevCall& C, const f2m_params& prm,
                                  std::vector<int32_t>& status, std::vector<double>& lp,
                                  std::vector<int32_t>* max_rank) {
@@ -989,15 +991,97 @@ static f2m_status complete_batch(f2m_ctx* ctx, DevCall& C, const f2m_params& prm
     for (int b = 0; b < C.pl.n_inst; ++b)
         if (status[b] == kNeedsHost) todo.push_back(b);
     if (todo.empty()) return F2M_OK;
+    const Batch& B = C.B;
+    const int ni = C.pl.n_inst;
+    std::vector<int32_t> Vn(ni);
+    std::vector<int64_t> offs(ni + 1);
+    std::vector<unsigned long long> db(ni);
+    F2M_CUDA(cudaMemcpyAsync(Vn.data(), B.Vn, ni * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(offs.data(), B.offs, (ni + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(db.data(), B.dmin_bits, ni * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    const size_t nt = todo.size();
+    std::vector<std::vector<int64_t>> rows(nt);
+    for (size_t k = 0; k < nt; ++k) {
+        const int b = todo[k];
+        rows[k].resize(Vn[b] + 1);
+        F2M_CUDA(cudaMemcpyAsync(rows[k].data(), B.row + offs[b], (Vn[b] + 1) * sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    // staging layout per instance: slots, cost, em, oth, mirror, perm | F, efcnt, ccnt, K
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    std::vector<size_t> off(nt + 1, 0);
+    for (size_t k = 0; k < nt; ++k) {
+        const int64_t V = Vn[todo[k]], S = rows[k][V] - rows[k][0];
+        off[k + 1] = off[k] + al(S * sizeof(Slot)) + al(S * 8) + 3 * al(S * 4) + al(S * 2) + al(V * 8) +
+                     3 * al(V * 4);
+    }
+    F2M_CUDA(ensure_pinned(ctx, off[nt]));
+    char* stage = ctx->pinned;
+    struct View {
+        Slot* slot; double* cost; int32_t* em; int32_t* oth; int32_t* mirror; uint16_t* perm;
+        double* F; int32_t* efcnt; int32_t* ccnt; int32_t* K;
+    };
+    std::vector<View> views(nt);
+    for (size_t k = 0; k < nt; ++k) {
+        const int b = todo[k];
+        const int64_t V = Vn[b], s0 = rows[k][0], S = rows[k][V] - s0, base = offs[b];
+        char* q = stage + off[k];
+        View& w = views[k];
+        auto take = [&](size_t bytes) { char* r = q; q += al(bytes); return r; };
+        w.slot = reinterpret_cast<Slot*>(take(S * sizeof(Slot)));
+        w.cost = reinterpret_cast<double*>(take(S * 8));
+        w.em = reinterpret_cast<int32_t*>(take(S * 4));
+        w.oth = reinterpret_cast<int32_t*>(take(S * 4));
+        w.mirror = reinterpret_cast<int32_t*>(take(S * 4));
+        w.perm = reinterpret_cast<uint16_t*>(take(S * 2));
+        w.F = reinterpret_cast<double*>(take(V * 8));
+        w.efcnt = reinterpret_cast<int32_t*>(take(V * 4));
+        w.ccnt = reinterpret_cast<int32_t*>(take(V * 4));
+        w.K = reinterpret_cast<int32_t*>(take(V * 4));
+        auto cp = [&](void* dst, const void* src, size_t bytes) {
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        };
+        F2M_CUDA(cp(w.slot, B.slot + s0, S * sizeof(Slot)));
+        F2M_CUDA(cp(w.cost, B.s_cost + s0, S * 8));
+        F2M_CUDA(cp(w.em, B.s_em + s0, S * 4));
+        F2M_CUDA(cp(w.oth, B.s_oth + s0, S * 4));
+        F2M_CUDA(cp(w.mirror, B.mirror + s0, S * 4));
+        F2M_CUDA(cp(w.perm, B.perm + s0, S * 2));
+        F2M_CUDA(cp(w.F, B.F + base, V * 8));
+        F2M_CUDA(cp(w.efcnt, B.efcnt + base, V * 4));
+        F2M_CUDA(cp(w.ccnt, B.ccnt + base, V * 4));
+        F2M_CUDA(cp(w.K, B.K + base, V * 4));
+    }
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
     std::mutex mu;
     std::atomic<size_t> next{0};
-    std::vector<f2m_status> err(todo.size(), F2M_OK);
+    std::vector<f2m_status> err(nt, F2M_OK);
     auto work = [&]() {
-        for (size_t k; (k = next.fetch_add(1)) < todo.size();) {
+        for (size_t k; (k = next.fetch_add(1)) < nt;) {
             const int b = todo[k];
+            const View& w = views[k];
             f2m_result R;
-            f2m_status s = pull_instance(ctx, C, b, R.H, true, &mu);
-            if (!s) s = complete_instance(ctx, C, b, prm, R, &mu);
+            HostInst& H = R.H;
+            const int V = Vn[b];
+            const int64_t s0 = rows[k][0], S = rows[k][V] - s0;
+            H.V = V;
+            std::memcpy(&H.dmin, &db[b], sizeof(double));
+            H.row.resize(V + 1);
+            for (int v = 0; v <= V; ++v) H.row[v] = rows[k][v] - s0;
+            H.nbr.resize(S);
+            H.Dn.resize(S);
+            for (int64_t a = 0; a < S; ++a) { H.nbr[a] = w.slot[a].nbr; H.Dn[a] = w.slot[a].D; }
+            H.cost.assign(w.cost, w.cost + S);
+            H.perm.assign(w.perm, w.perm + S);
+            H.mirror.assign(w.mirror, w.mirror + S);
+            H.F.assign(w.F, w.F + V);
+            H.efcnt.assign(w.efcnt, w.efcnt + V);
+            H.ccnt.assign(w.ccnt, w.ccnt + V);
+            H.label.assign(w.K, w.K + V);
+            number_edges(H, std::vector<int>(w.em, w.em + S), std::vector<int>(w.oth, w.oth + S));
+            const f2m_status s = complete_instance(ctx, C, b, prm, R, &mu);
             err[k] = s;
             if (s) continue;
             status[b] = R.status;
@@ -1006,9 +1090,9 @@ static f2m_status complete_batch(f2m_ctx* ctx, DevCall& C, const f2m_params& prm
         }
     };
     const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t nt = std::min(todo.size(), std::min<size_t>(hw, 32));
+    const size_t nthr = std::min(nt, std::min<size_t>(hw, 32));
     std::vector<std::thread> pool;
-    for (size_t t = 1; t < nt; ++t) pool.emplace_back(work);
+    for (size_t t = 1; t < nthr; ++t) pool.emplace_back(work);
     work();
     for (auto& t : pool) t.join();
     for (f2m_status s : err)
