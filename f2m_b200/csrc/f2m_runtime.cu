@@ -310,13 +310,69 @@ struct HostInst {
 
 // Edge ids in the reference's global order: slots with nbr>v, sorted by the
 // candidate key (cost, emitter, partner) (FXY.hpp:100-101, graph_tour.hpp:28-90).
+// fn(begin, end) over [0, n) in contiguous ranges on up to 32 host threads
+// (inline below 20,000 items)
+template <class Fn>
+void parallel_for(int64_t n, Fn fn) {
+    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t T = (n < 20000) ? 1 : std::min<int64_t>(std::min<int64_t>(hw, 32), n);
+    if (T <= 1) { fn((int64_t)0, n); return; }
+    std::vector<std::thread> pool;
+    for (int64_t t = 1; t < T; ++t) pool.emplace_back(fn, n * t / T, n * (t + 1) / T);
+    fn((int64_t)0, n / T);
+    for (auto& th : pool) th.join();
+}
+
+// std::sort of a large array as sorted chunks merged pairwise, each level's
+// merges side by side (the keys here are unique, so the order is the same)
+template <class T, class Less>
+void parallel_sort(std::vector<T>& a, Less less) {
+    const int64_t n = (int64_t)a.size();
+    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    int64_t parts = 1;
+    while (parts * 2 <= std::min<int64_t>(hw, 32)) parts *= 2;
+    if (n < 200000 || parts < 2) { std::sort(a.begin(), a.end(), less); return; }
+    std::vector<int64_t> b(parts + 1);
+    for (int64_t p = 0; p <= parts; ++p) b[p] = n * p / parts;
+    parallel_for(parts * 20000, [&](int64_t i0, int64_t i1) {
+        for (int64_t p = i0 / 20000; p < (i1 + 19999) / 20000 && p < parts; ++p)
+            if (p * 20000 >= i0) std::sort(a.begin() + b[p], a.begin() + b[p + 1], less);
+    });
+    std::vector<T> tmp(n);
+    for (int64_t w = 1; w < parts; w *= 2) {
+        const int64_t pairs = parts / (2 * w);
+        std::vector<std::thread> pool;
+        for (int64_t q = 0; q < pairs; ++q)
+            pool.emplace_back([&, q] {
+                const int64_t l = b[2 * w * q], m = b[2 * w * q + w], r = b[2 * w * (q + 1)];
+                std::merge(a.begin() + l, a.begin() + m, a.begin() + m, a.begin() + r, tmp.begin() + l, less);
+            });
+        for (auto& th : pool) th.join();
+        a.swap(tmp);
+    }
+}
+
 void number_edges(HostInst& H, const std::vector<int>& em, const std::vector<int>& oth) {
     struct K { double c; int e, o; int v; int64_t s; };
-    std::vector<K> ks;
-    for (int v = 0; v < H.V; ++v)
-        for (int64_t a = H.row[v]; a < H.row[v + 1]; ++a)
-            if (H.nbr[a] > v) ks.push_back({H.cost[a], em[a], oth[a], v, a});
-    std::sort(ks.begin(), ks.end(), [](const K& x, const K& y) {
+    // slots with nbr > v, numbered per node, filled side by side
+    std::vector<int64_t> first(H.V + 1, 0);
+    parallel_for(H.V, [&](int64_t v0, int64_t v1) {
+        for (int64_t v = v0; v < v1; ++v) {
+            int64_t c = 0;
+            for (int64_t a = H.row[v]; a < H.row[v + 1]; ++a) c += H.nbr[a] > v;
+            first[v + 1] = c;
+        }
+    });
+    for (int v = 0; v < H.V; ++v) first[v + 1] += first[v];
+    std::vector<K> ks(first[H.V]);
+    parallel_for(H.V, [&](int64_t v0, int64_t v1) {
+        for (int64_t v = v0; v < v1; ++v) {
+            int64_t q = first[v];
+            for (int64_t a = H.row[v]; a < H.row[v + 1]; ++a)
+                if (H.nbr[a] > v) ks[q++] = K{H.cost[a], em[a], oth[a], (int)v, a};
+        }
+    });
+    parallel_sort(ks, [](const K& x, const K& y) {
         if (x.c != y.c) return x.c < y.c;
         if (x.e != y.e) return x.e < y.e;
         return x.o < y.o;
@@ -325,7 +381,8 @@ void number_edges(HostInst& H, const std::vector<int>& em, const std::vector<int
     H.slot_edge.assign(H.nbr.size(), -1);
     H.ev1.resize(H.E); H.ev2.resize(H.E); H.el1.resize(H.E); H.el2.resize(H.E);
     H.rank1.resize(H.E); H.rank2.resize(H.E); H.eD.resize(H.E); H.eDo.resize(H.E);
-    for (int e = 0; e < H.E; ++e) {
+    parallel_for(H.E, [&](int64_t e0, int64_t e1) {
+    for (int64_t e = e0; e < e1; ++e) {
         const int v = ks[e].v;
         const int64_t a = ks[e].s;
         const int u = H.nbr[a];
@@ -337,6 +394,7 @@ void number_edges(HostInst& H, const std::vector<int>& em, const std::vector<int
         if (H.label[v] < H.label[u]) { H.el1[e] = v; H.el2[e] = u; H.rank1[e] = rv; H.rank2[e] = ru; }
         else { H.el1[e] = u; H.el2[e] = v; H.rank1[e] = ru; H.rank2[e] = rv; }
     }
+    });
 }
 
 struct HostCheck {
@@ -356,8 +414,10 @@ struct HostCheck {
 
     HostCheck(HostInst& h, double band) : H(h), vb(band) {
         node_edges.resize(H.V);
-        for (int v = 0; v < H.V; ++v)
-            for (int64_t a = H.row[v]; a < H.row[v + 1]; ++a) node_edges[v].push_back(H.slot_edge[a]);
+        parallel_for(H.V, [&](int64_t v0, int64_t v1) {
+            for (int64_t v = v0; v < v1; ++v)
+                node_edges[v].assign(H.slot_edge.begin() + H.row[v], H.slot_edge.begin() + H.row[v + 1]);
+        });
     }
     double dgpu(int64_t a, int v) const {  // cuda_recompute_Edges
         const int u = H.nbr[a];
@@ -462,22 +522,26 @@ struct HostCheck {
     int check() {
         const int E = H.E;
         std::vector<double> dcpu(E);
-        for (int e = 0; e < E; ++e)  // E_thread.cpp:39
-            dcpu[e] = H.eD[e] + H.F[H.el1[e]] / 2 + H.F[H.el2[e]] / 2;
+        parallel_for(E, [&](int64_t e0, int64_t e1) {
+            for (int64_t e = e0; e < e1; ++e)  // E_thread.cpp:39
+                dcpu[e] = H.eD[e] + H.F[H.el1[e]] / 2 + H.F[H.el2[e]] / 2;
+        });
         eA.assign(H.V, {});
         eB.assign(H.V, {});
         sA.assign(H.V, 0);
         sB.assign(H.V, 0);
-        for (int v = 0; v < H.V; ++v) {  // node::resort + node::get_statusAB
-            auto& ed = node_edges[v];
-            std::sort(ed.begin(), ed.end(), [&](int a, int b) { return dcpu[a] < dcpu[b]; });
-            for (int e : ed) {
-                if (dcpu[e] < vb) {
-                    if (dcpu[e] > -vb) { sB[v]++; eB[v].push_back(e); }
-                    else { sA[v]++; eA[v].push_back(e); }
-                } else break;
+        parallel_for(H.V, [&](int64_t v0, int64_t v1) {
+            for (int64_t v = v0; v < v1; ++v) {  // node::resort + node::get_statusAB
+                auto& ed = node_edges[v];
+                std::sort(ed.begin(), ed.end(), [&](int a, int b) { return dcpu[a] < dcpu[b]; });
+                for (int e : ed) {
+                    if (dcpu[e] < vb) {
+                        if (dcpu[e] > -vb) { sB[v]++; eB[v].push_back(e); }
+                        else { sA[v]++; eA[v].push_back(e); }
+                    } else break;
+                }
             }
-        }
+        });
         extract_combs();
         Combs.clear();
         Combs.resize(comb_V.size());
@@ -666,8 +730,8 @@ f2m_status h2d(f2m_ctx* ctx, T* dst, const std::vector<T>& v) {
 }
 
 // Pull instance b (device-built graph, node ids = de-duplicated input order).
-// Copies instance b to the host.  `mu` (optional) serialises the stream work
-// when several host threads complete instances of one call.
+// Copies instance b to the host (through pinned staging, one synchronisation
+// for the bulk arrays).  `mu` (optional) serialises the stream work.
 f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, bool with_keys,
                          std::mutex* mu = nullptr) {
     std::unique_lock<std::mutex> lk;
@@ -686,37 +750,60 @@ f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, boo
     if (d2h(ctx, row, B.row + base, V + 1)) return F2M_ERR_CUDA;
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
     const int64_t s0 = row[0], S = row[V] - row[0];
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t bytes = al(S * sizeof(Slot)) + al(S * 8) + 3 * al(S * 4) + al(S * 2) + al(V * 8) + 3 * al(V * 4);
+    F2M_CUDA(ensure_pinned(ctx, bytes));
+    char* q = ctx->pinned;
+    auto take = [&](size_t n) { char* r = q; q += al(n); return r; };
+    Slot* sl = reinterpret_cast<Slot*>(take(S * sizeof(Slot)));
+    double* cost = reinterpret_cast<double*>(take(S * 8));
+    int32_t* em = reinterpret_cast<int32_t*>(take(S * 4));
+    int32_t* oth = reinterpret_cast<int32_t*>(take(S * 4));
+    int32_t* mirror = reinterpret_cast<int32_t*>(take(S * 4));
+    uint16_t* perm = reinterpret_cast<uint16_t*>(take(S * 2));
+    double* F = reinterpret_cast<double*>(take(V * 8));
+    int32_t* efcnt = reinterpret_cast<int32_t*>(take(V * 4));
+    int32_t* ccnt = reinterpret_cast<int32_t*>(take(V * 4));
+    int32_t* K = reinterpret_cast<int32_t*>(take(V * 4));
+    auto cp = [&](void* dst, const void* src, size_t n) {
+        return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->stream);
+    };
+    F2M_CUDA(cp(sl, B.slot + s0, S * sizeof(Slot)));
+    F2M_CUDA(cp(cost, B.s_cost + s0, S * 8));
+    F2M_CUDA(cp(mirror, B.mirror + s0, S * 4));
+    F2M_CUDA(cp(perm, B.perm + s0, S * 2));
+    if (with_keys) {
+        F2M_CUDA(cp(em, B.s_em + s0, S * 4));
+        F2M_CUDA(cp(oth, B.s_oth + s0, S * 4));
+    }
+    F2M_CUDA(cp(F, B.F + base, V * 8));
+    F2M_CUDA(cp(efcnt, B.efcnt + base, V * 4));
+    F2M_CUDA(cp(ccnt, B.ccnt + base, V * 4));
+    F2M_CUDA(cp(K, B.K + base, V * 4));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
     H.row.resize(V + 1);
     for (int v = 0; v <= V; ++v) H.row[v] = row[v] - s0;
-    std::vector<Slot> sl;
-    std::vector<int> em, oth;
-    f2m_status s = F2M_OK;
-    if ((s = d2h(ctx, sl, B.slot + s0, S))) return s;
-    if ((s = d2h(ctx, H.cost, B.s_cost + s0, S))) return s;
-    if ((s = d2h(ctx, H.perm, B.perm + s0, S))) return s;
-    if ((s = d2h(ctx, H.mirror, B.mirror + s0, S))) return s;
-    if ((s = d2h(ctx, H.F, B.F + base, V))) return s;
-    if ((s = d2h(ctx, H.efcnt, B.efcnt + base, V))) return s;
-    if ((s = d2h(ctx, H.ccnt, B.ccnt + base, V))) return s;
-    if ((s = d2h(ctx, H.label, B.K + base, V))) return s;
-    if (with_keys) {
-        if ((s = d2h(ctx, em, B.s_em + s0, S))) return s;
-        if ((s = d2h(ctx, oth, B.s_oth + s0, S))) return s;
-    }
-    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (lk.owns_lock()) lk.unlock();
     H.nbr.resize(S);
     H.Dn.resize(S);
-    for (int64_t a = 0; a < S; ++a) { H.nbr[a] = sl[a].nbr; H.Dn[a] = sl[a].D; }
+    parallel_for(S, [&](int64_t a0, int64_t a1) {
+        for (int64_t a = a0; a < a1; ++a) { H.nbr[a] = sl[a].nbr; H.Dn[a] = sl[a].D; }
+    });
+    H.cost.assign(cost, cost + S);
+    H.perm.assign(perm, perm + S);
+    H.mirror.assign(mirror, mirror + S);
+    H.F.assign(F, F + V);
+    H.efcnt.assign(efcnt, efcnt + V);
+    H.ccnt.assign(ccnt, ccnt + V);
+    H.label.assign(K, K + V);
     if (with_keys) {
+        std::vector<int> ev(em, em + S), ov(oth, oth + S);
+        if (lk.owns_lock()) lk.unlock();  // the staging is no longer needed
         // keys hold FXY indices; node ids here are the same indices
-        number_edges(H, em, oth);
+        number_edges(H, ev, ov);
     }
     return F2M_OK;
 }
 
-// graph::RUN after the descent (graph_cuda.cu:64-153) for one instance:
-// host comb check, repair loop through device refits, primal and report values.
 f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& prm, f2m_result& R,
                              std::mutex* mu = nullptr) {
     HostInst& H = R.H;
