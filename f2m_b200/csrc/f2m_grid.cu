@@ -18,7 +18,7 @@
 
 namespace f2m {
 
-constexpr int kGT = 512;               // threads per CTA
+constexpr int kGT = 1024;              // threads per CTA (one CTA per SM: fewer barrier arrivals)
 constexpr long long kSpinLimit = 1LL << 26;  // ~seconds of waiting before giving up
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -415,7 +415,7 @@ struct GridSolver {
     }
 };
 
-__global__ void __launch_bounds__(kGT, 2) k_solve_grid(Batch B, DevParams P, GridState G, int b, int refit,
+__global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, GridState G, int b, int refit,
                                                      int cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sred[kGT / 32];
