@@ -61,6 +61,11 @@ struct f2m_ctx {
     Batch last{};  // pointers of the last batched call (for the work counters)
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
+    // CUDA graph of the smoothed bound's per-step launches, replayed while the
+    // call's shape (sizes, parameters, arena) repeats
+    cudaGraphExec_t sgraph = nullptr;
+    std::vector<int64_t> skey;
+    int64_t sgraph_launches = 0;
 };
 
 namespace {
@@ -1014,6 +1019,7 @@ void f2m_destroy(f2m_ctx* c) {
         if (c->join[k]) cudaEventDestroy(c->join[k]);
     }
     if (c->fork) cudaEventDestroy(c->fork);
+    if (c->sgraph) cudaGraphExecDestroy(c->sgraph);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -1404,6 +1410,43 @@ void f2m_get_class_bounds(int32_t* max_nodes) { solve_get_bounds(max_nodes); }
 
 namespace {
 
+// The per-step launches (4 x iters + a few) as one CUDA graph: captured on
+// the first call of a shape and replayed while the shape repeats (all kernel
+// arguments are sizes, parameters and arena pointers, which the key covers;
+// the data they point to is written before each replay).
+cudaError_t smooth_steps_graph(f2m_ctx* ctx, SmoothBatch& B, bool grad) {
+    int64_t tb, ob;
+    std::memcpy(&tb, &B.tau, 8);
+    std::memcpy(&ob, &B.omega, 8);
+    const std::vector<int64_t> key{B.n_total, B.n_inst, B.N, B.iters, B.ckpt, B.newton_max, grad ? 1 : 0,
+                                   tb, ob, (int64_t)(intptr_t)ctx->dev, (int64_t)ctx->dev_cap};
+    if (ctx->sgraph && key == ctx->skey) {
+        ctx->launches += ctx->sgraph_launches;
+        return cudaGraphLaunch(ctx->sgraph, ctx->stream);
+    }
+    if (ctx->sgraph) {
+        cudaGraphExecDestroy(ctx->sgraph);
+        ctx->sgraph = nullptr;
+    }
+    cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    int64_t n = 0;
+    const cudaError_t el = launch_smooth_steps(B, grad, ctx->stream, &n);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(ctx->stream, &g);
+    if (el != cudaSuccess) e = el;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->sgraph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        ctx->sgraph = nullptr;
+        return e;
+    }
+    ctx->skey = key;
+    ctx->sgraph_launches = n;
+    ctx->launches += n;
+    return cudaGraphLaunch(ctx->sgraph, ctx->stream);
+}
+
 // Shared body of the smoothed-bound entry points: buffers from the context's
 // arena, host inputs copied in, graph + bound (+ adjoint) on the device.
 f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const float* x,
@@ -1500,7 +1543,7 @@ f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const 
     F2M_CUDA(cudaMemcpyAsync(dLd, up.data(), n_inst * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(launch_smooth_graph(B, scan, ctx->stream, &ctx->launches));
     B.solver = steps ? 2 : 1;
-    if (steps) F2M_CUDA(launch_smooth_steps(B, grad, ctx->stream, &ctx->launches));
+    if (steps) F2M_CUDA(smooth_steps_graph(ctx, B, grad));
     else F2M_CUDA(launch_smooth_bound(B, max_v, grad, ctx->stream, &ctx->launches));
     F2M_CUDA(cudaMemcpyAsync(L, B.L, n_inst * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (gx) F2M_CUDA(cudaMemcpyAsync(gx, B.gx, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));

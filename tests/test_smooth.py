@@ -120,3 +120,23 @@ def test_smooth_input_errors_without_device():
     import f2m_b200
     with pytest.raises(f2m_b200.F2MError):
         f2m_b200.Context(0).smoothed_bound(np.array([0, 3]), np.zeros(3), np.zeros(3), 3)
+
+
+@pytest.mark.gpu
+def test_per_step_graph_replay_reads_new_inputs(ctx):
+    """The per-step launches are replayed from a CUDA graph while the call's
+    shape repeats; a replay must see the new points."""
+    import f2m_b200
+    p = f2m_b200.default_smooth_params(tau=1e-2, iters=20, solver=2)
+    offs = np.array([0, 500], np.int64)
+    x1, y1 = synth.config4(1, 500)
+    x2, y2 = synth.config4(2, 500)
+    La, ga, _ = ctx.smoothed_bound(offs, x1, y1, 12, params=p, grad=True)
+    Lb, gb, _ = ctx.smoothed_bound(offs, x2, y2, 12, params=p, grad=True)  # replay
+    fresh = f2m_b200.Context(0)
+    try:
+        Lc, gc, _ = fresh.smoothed_bound(offs, x2, y2, 12, params=p, grad=True)
+    finally:
+        fresh.close()
+    assert La[0] != Lb[0]
+    assert Lb[0] == Lc[0] and np.array_equal(gb, gc)
