@@ -245,3 +245,40 @@ def test_class_bounds_change_speed_not_results(ctx):
     # order follows the team size
     assert np.array_equal(st0, st1)
     assert np.all(np.abs(lp0 - lp1) <= LP_RTOL * np.abs(lp0))
+
+
+def test_batch_edge_cases_match_oracle(ctx, oracle):
+    """Ragged batch: instances of 4-12 points (N clamped to V-1), repeated and
+    collinear points, one all-identical instance (an input error), and one
+    instance of 10,000 points (the largest the batched solver takes)."""
+    parts = []
+    for n in (4, 5, 6, 8, 12):
+        parts.append(synth.uniform_int_points(n, 100 + n))
+    parts.append((np.array([0, 0, 0, 1, 1, 2, 2, 3, 5, 8], float),
+                  np.array([0, 0, 0, 1, 1, 2, 2, 3, 5, 8], float)))
+    x, y = synth.uniform_int_points(30, 7)
+    parts.append((np.concatenate([x, x]), np.concatenate([y, y])))
+    parts.append((np.zeros(10), np.zeros(10)))
+    parts.append(synth.uniform_int_points(10000, 99))
+    offs = np.concatenate([[0], np.cumsum([len(p[0]) for p in parts])]).astype(np.int64)
+    X = np.concatenate([p[0] for p in parts])
+    Y = np.concatenate([p[1] for p in parts])
+    lp, st = ctx.solve_batch(offs, X, Y, 16)
+    lp_o, st_o, _ = oracle.solve_batch(offs, X, Y, 16, threads=os.cpu_count() or 1)
+    assert np.array_equal(st, st_o)
+    assert st[7] == f2m_b200.ERR_INPUT
+    ok = st_o == 0
+    assert ok.sum() == len(parts) - 1
+    assert np.all(np.abs(lp[ok] - lp_o[ok]) <= LP_RTOL * np.abs(lp_o[ok]))
+
+
+def test_batch_argument_errors(ctx):
+    with pytest.raises(f2m_b200.F2MError) as e:
+        ctx.solve_batch(np.array([0], np.int64), np.zeros(0), np.zeros(0), 16)
+    assert e.value.status == f2m_b200.ERR_INPUT
+    with pytest.raises(f2m_b200.F2MError) as e:
+        ctx.solve_batch(np.array([0, 50], np.int64), *synth.uniform_int_points(50, 1), 300)
+    assert e.value.status == f2m_b200.ERR_CAPACITY
+    with pytest.raises(f2m_b200.F2MError) as e:
+        ctx.solve_batch(np.array([0, 60, 40], np.int64), *synth.uniform_int_points(60, 1), 8)
+    assert e.value.status == f2m_b200.ERR_INPUT
