@@ -1386,6 +1386,137 @@ f2m_status f2m_knn(f2m_ctx* ctx, const double* x, const double* y, const int32_t
     return points_call(ctx, x, y, labels, n, top_k, nullptr, false, out);
 }
 
+// graph_c(graph*) + graph::RUN() (F2M.h:175,320) on a graph the caller built:
+// edges in edge-id order, per-node lists in that order (graph_cuda_init.hpp:
+// 42-63), D as given, d_min = the smallest Do (graph_tour.hpp:70).
+f2m_status f2m_solve_graph(f2m_ctx* ctx, int32_t n_nodes, int32_t n_edges, const int32_t* v1,
+                           const int32_t* v2, const double* D, const double* Do, const int32_t* labels,
+                           const f2m_params* params, f2m_result** out) {
+    *out = nullptr;
+    if (!ctx) return F2M_ERR_INPUT;
+    if (n_nodes < 4 || n_edges < 1 || !v1 || !v2 || !D || !Do)
+        return fail(ctx, F2M_ERR_INPUT, "need at least 4 nodes and 1 edge");
+    f2m_params prm;
+    f2m_default_params(&prm);
+    if (params) prm = *params;
+    std::vector<int64_t> row(n_nodes + 1, 0);
+    double dmin = INFINITY;
+    for (int32_t e = 0; e < n_edges; ++e) {
+        const int a = v1[e], b = v2[e];
+        if (a < 0 || b < 0 || a >= n_nodes || b >= n_nodes || a == b || !(Do[e] > 0) || !(D[e] > 0))
+            return fail(ctx, F2M_ERR_INPUT, "edge " + std::to_string(e) + " is invalid");
+        row[a + 1]++;
+        row[b + 1]++;
+        dmin = std::min(dmin, Do[e]);
+    }
+    int64_t maxdeg = 0;
+    for (int32_t v = 0; v < n_nodes; ++v) {
+        maxdeg = std::max(maxdeg, row[v + 1]);
+        row[v + 1] += row[v];
+    }
+    if (maxdeg > 65535) return fail(ctx, F2M_ERR_CAPACITY, "a node has more than 65535 edges");
+    const int64_t S = row[n_nodes];
+    cudaSetDevice(ctx->device);
+    std::unique_ptr<f2m_result> R(new f2m_result());
+    HostInst& H = R->H;
+    H.V = n_nodes;
+    H.E = n_edges;
+    H.dmin = dmin;
+    H.row = row;
+    H.nbr.resize(S);
+    H.Dn.resize(S);
+    H.cost.resize(S);
+    H.mirror.resize(S);
+    H.slot_edge.resize(S);
+    H.ev1.resize(n_edges); H.ev2.resize(n_edges); H.el1.resize(n_edges); H.el2.resize(n_edges);
+    H.rank1.resize(n_edges); H.rank2.resize(n_edges);
+    H.eD.assign(D, D + n_edges);
+    H.eDo.assign(Do, Do + n_edges);
+    H.label.resize(n_nodes);
+    for (int32_t v = 0; v < n_nodes; ++v) H.label[v] = labels ? labels[v] : v + 1;
+    std::vector<int64_t> fill(row.begin(), row.end() - 1);
+    std::vector<Slot> slots(S);
+    for (int32_t e = 0; e < n_edges; ++e) {
+        const int a = std::min(v1[e], v2[e]), b = std::max(v1[e], v2[e]);
+        const int64_t sa = fill[a]++, sb = fill[b]++;
+        const int ra = (int)(sa - row[a]), rb = (int)(sb - row[b]);
+        H.nbr[sa] = b; H.nbr[sb] = a;
+        H.Dn[sa] = H.Dn[sb] = D[e];
+        H.cost[sa] = H.cost[sb] = Do[e];
+        H.mirror[sa] = rb; H.mirror[sb] = ra;
+        H.slot_edge[sa] = H.slot_edge[sb] = e;
+        H.ev1[e] = a; H.ev2[e] = b;
+        if (H.label[a] < H.label[b]) { H.el1[e] = a; H.el2[e] = b; H.rank1[e] = ra; H.rank2[e] = rb; }
+        else { H.el1[e] = b; H.el2[e] = a; H.rank1[e] = rb; H.rank2[e] = ra; }
+        slots[sa] = Slot{D[e], b, ra};
+        slots[sb] = Slot{D[e], a, rb};
+    }
+    std::vector<uint16_t> perm(S);
+    for (int32_t v = 0; v < n_nodes; ++v)
+        for (int64_t q = row[v]; q < row[v + 1]; ++q) perm[q] = (uint16_t)(q - row[v]);
+    // device buffers of one instance; the list capacity follows the degrees
+    const int64_t offs[2] = {0, n_nodes};
+    const int32_t cap_n = (int32_t)std::min<int64_t>(256, std::max<int64_t>(3, (S + n_nodes - 1) / n_nodes + 1));
+    DevCall C;
+    f2m_status st = setup_call(ctx, C, 1, offs, cap_n, prm, true);
+    if (st) return st;
+    if (C.B.S_cap < S) return fail(ctx, F2M_ERR_CAPACITY, "graph too dense for the solver's list arrays");
+    Batch& B = C.B;
+    std::vector<int32_t> mirror32(H.mirror.begin(), H.mirror.end());
+    const int32_t one_v = n_nodes, ok = F2M_OK;
+    unsigned long long db;
+    std::memcpy(&db, &dmin, sizeof(db));
+    std::vector<double> zeros(n_nodes, 0.0);
+    auto h2 = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    };
+    F2M_CUDA(h2(const_cast<int64_t*>(B.offs), offs, sizeof(offs)));
+    F2M_CUDA(h2(B.Vn, &one_v, sizeof(one_v)));
+    F2M_CUDA(h2(B.status, &ok, sizeof(ok)));
+    F2M_CUDA(h2(B.dmin_bits, &db, sizeof(db)));
+    F2M_CUDA(h2(B.row, row.data(), row.size() * sizeof(int64_t)));
+    F2M_CUDA(h2(B.slot, slots.data(), S * sizeof(Slot)));
+    F2M_CUDA(h2(B.perm, perm.data(), S * sizeof(uint16_t)));
+    F2M_CUDA(h2(B.mirror, mirror32.data(), S * sizeof(int32_t)));
+    F2M_CUDA(h2(B.s_cost, H.cost.data(), S * sizeof(double)));
+    F2M_CUDA(h2(B.K, H.label.data(), n_nodes * sizeof(int32_t)));
+    F2M_CUDA(h2(const_cast<double*>(B.shift), zeros.data(), n_nodes * sizeof(double)));
+    auto t0 = std::chrono::steady_clock::now();
+    F2M_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+    F2M_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+    F2M_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
+    F2M_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+    f2m_status s = launch_classes(ctx, C, prm);
+    if (s) return s;
+    F2M_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
+    ctx->timed = true;
+    ctx->last = C.B;
+    int32_t stt = 0;
+    F2M_CUDA(cudaMemcpyAsync(&stt, B.status, sizeof(stt), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (stt != F2M_OK && stt != kNeedsHost) {
+        R->status = stt;
+        R->err = "instance exceeds a solver limit or did not converge";
+        *out = R.release();
+        return (f2m_status)stt;
+    }
+    H.perm.resize(S);
+    H.F.resize(n_nodes);
+    H.efcnt.resize(n_nodes);
+    H.ccnt.resize(n_nodes);
+    F2M_CUDA(cudaMemcpyAsync(H.perm.data(), B.perm, S * sizeof(uint16_t), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(H.F.data(), B.F, n_nodes * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(H.efcnt.data(), B.efcnt, n_nodes * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(H.ccnt.data(), B.ccnt, n_nodes * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if ((s = pull_stats(ctx, C, 0, *R))) return s;
+    if ((s = complete_instance(ctx, C, 0, prm, *R))) return s;
+    if ((s = pull_stats(ctx, C, 0, *R))) return s;
+    R->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = R.release();
+    return (f2m_status)(*out)->status;
+}
+
 /* ------------------------------------------------------------------ */
 /* smoothed bound (f2m_smooth.cu)                                       */
 /* ------------------------------------------------------------------ */

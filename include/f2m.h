@@ -136,6 +136,16 @@ typedef struct f2m_result f2m_result;
 f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y,
                             const int32_t* labels, int32_t n, int32_t top_k,
                             const f2m_params* params, f2m_result** out);
+/* graph_c(graph*) + graph::RUN() (F2M.h:175,320) on a graph the caller
+ * built: n_edges edges between node indices v1/v2 (either order) in the
+ * reference's edge order (graph::E, ascending Do, graph_tour.hpp:28-98),
+ * each node's list in that order (graph_cuda_init.hpp:42-63), normalised
+ * costs D (Do / d_min) and raw costs Do; labels (n_nodes, NULL = 1..n) name
+ * the nodes in the outputs.  Solves on the device and runs the host comb
+ * stage, as f2m_solve_points. */
+f2m_status f2m_solve_graph(f2m_ctx* ctx, int32_t n_nodes, int32_t n_edges, const int32_t* v1,
+                           const int32_t* v2, const double* D, const double* Do,
+                           const int32_t* labels, const f2m_params* params, f2m_result** out);
 /* The kNN graph alone: FXY's candidate kNN (FXY.hpp:23-144, 313-534) and the
  * greedy union of graph::graph (graph_tour.hpp:28-98), without solving.  The
  * result carries the edges in the reference's edge order

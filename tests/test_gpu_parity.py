@@ -282,3 +282,21 @@ def test_batch_argument_errors(ctx):
     with pytest.raises(f2m_b200.F2MError) as e:
         ctx.solve_batch(np.array([0, 60, 40], np.int64), *synth.uniform_int_points(60, 1), 8)
     assert e.value.status == f2m_b200.ERR_INPUT
+
+
+def test_solve_graph_matches_oracle(ctx, oracle):
+    """graph_c + RUN on a caller-built graph (here the oracle's kNN graph),
+    including a lattice graph that needs the repair loop."""
+    cases = [(synth.uniform_int_points(900, 61), 12), (synth.lattice_points(300, 2), 8)]
+    for (x, y), N in cases:
+        g = oracle.build_graph(x, y, N)
+        o = oracle.solve_graph(g.n_nodes, g.v1, g.v2, g.D, g.Do, label=g.label)
+        r = ctx.solve_graph(g.n_nodes, g.v1, g.v2, g.D, g.Do, labels=g.label)
+        assert r.status == o.status
+        assert np.array_equal(r.F, o.F), "potentials differ from the oracle"
+        if o.status == 0:
+            assert _close(r.lp, o.lp)
+            assert r.max_rank == o.max_rank
+            assert np.array_equal(r.x, o.x)
+        p = ctx.solve_points(x, y, N)  # the same graph through the points path
+        assert np.array_equal(p.F, r.F)
