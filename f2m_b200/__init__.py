@@ -90,7 +90,7 @@ EXPORTS = [
     "f2m_result_edges", "f2m_result_nodes", "f2m_result_stats", "f2m_phase_times",
     "f2m_solve_points_noalloc", "f2m_default_smooth_params", "f2m_smoothed_bound_fwd",
     "f2m_smoothed_bound_bwd", "f2m_smooth_max_nodes", "f2m_knn", "f2m_set_class_bounds",
-    "f2m_get_class_bounds", "f2m_solve_graph",
+    "f2m_get_class_bounds", "f2m_solve_graph", "f2m_solve_points_from",
 ]
 
 _lib = None
@@ -117,6 +117,7 @@ def lib():
         L.f2m_solve_batch_device.argtypes = [vp, i32, vp, vp, vp, vp, i32, P(Params), P(BatchOut)]
         L.f2m_solve_points.argtypes = [vp, vp, vp, vp, i32, i32, P(Params), P(vp)]
         L.f2m_knn.argtypes = [vp, vp, vp, vp, i32, i32, P(vp)]
+        L.f2m_solve_points_from.argtypes = [vp, vp, vp, vp, i32, i32, vp, i32, P(Params), P(vp)]
         L.f2m_solve_graph.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp, P(Params), P(vp)]
         L.f2m_solve_file.argtypes = [vp, ctypes.c_char_p, i32, P(Params), i32, P(vp)]
         L.f2m_result_free.argtypes = [vp]
@@ -306,6 +307,18 @@ class Context:
         p = params if params is not None else default_params()
         s = lib().f2m_solve_graph(self._h, int(n_nodes), len(v1), _ptr(v1), _ptr(v2), _ptr(D), _ptr(Do),
                                   _ptr(lab), ctypes.byref(p), ctypes.byref(h))
+        return self._result(s, h)
+
+    def solve_points_from(self, x, y, top_k, F0, labels=None, params=None):
+        """Resume the descent from stored potentials F0 (node order of a result)."""
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        F0 = np.ascontiguousarray(F0, np.float64)
+        lab = None if labels is None else np.ascontiguousarray(labels, np.int32)
+        h = ctypes.c_void_p()
+        p = params if params is not None else default_params()
+        s = lib().f2m_solve_points_from(self._h, _ptr(x), _ptr(y), _ptr(lab), len(x), top_k, _ptr(F0),
+                                        len(F0), ctypes.byref(p), ctypes.byref(h))
         return self._result(s, h)
 
     def knn(self, x, y, top_k, labels=None):

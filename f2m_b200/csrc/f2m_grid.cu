@@ -435,9 +435,9 @@ __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, Gri
     GridSolver S{B, P, G, I, b, v0, v1, I.row[0], G.Ha, G.Hb, eD, eW, cap, sefo, sred, sredl, swarp, sbc, sflag};
     double M;
     if (!refit) {
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) G.Ha[v] = 0.0;  // F = 0
+        for (int v = v0 + threadIdx.x; v < v1; v += kGT) G.Ha[v] = B.F0 ? 0.5 * B.F0[I.base + v] : 0.0;  // F = 0 or warm
         S.sync();
-        M = S.run_start();
+        M = B.F0 ? S.run_fix() : S.run_start();  // a resumed descent skips the global phase
     } else {
         // cuda_IRREGULAR_B_recompute (graph_cuda_comb.hpp:542-574)
         for (int v = v0 + threadIdx.x; v < v1; v += kGT) {

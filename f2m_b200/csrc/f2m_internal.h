@@ -99,6 +99,7 @@ struct Batch {
     int32_t* efcnt;         // [n_total] EF list length (cuda_EF_NodesStat)
     int32_t* ccnt;          // [n_total] comb prefix length (cuda_COMB_NodesStat)
     const double* shift;    // [n_total] repair shift per node (k_refit input; 0 = none)
+    const double* F0;       // [n_total] starting potentials (warm start), or null for F = 0
     // per-instance results
     double* lp;
     int32_t* n_edges;

@@ -1252,9 +1252,12 @@ __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, con
         Solver<TEAM> S(B, P, I, T, M);
         double Mg;
         if (!REFIT) {
-            for (int v = T.tid; v < I.V; v += TEAM) M.Ha[v] = 0.0;  // F = 0, graph_cuda_init.hpp:183
+            // F = 0 (graph_cuda_init.hpp:183), or a warm start
+            // (resuming from given potentials skips the global phase: run_fix,
+            // the schedule the reference runs after a repair shift)
+            for (int v = T.tid; v < I.V; v += TEAM) M.Ha[v] = B.F0 ? 0.5 * B.F0[I.base + v] : 0.0;
             T.sync();
-            Mg = S.run_start();
+            Mg = B.F0 ? S.run_fix() : S.run_start();
         } else {
             // cuda_IRREGULAR_B_recompute (graph_cuda_comb.hpp:542-574): shift the
             // potentials of irregular combs, 20 frozen iterations, run_fix; the

@@ -23,6 +23,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "f2m_internal.h"
 
 using namespace f2m;
@@ -31,6 +33,13 @@ using namespace f2m;
 /* context                                                              */
 /* ------------------------------------------------------------------ */
 namespace {
+
+// NVTX range for the lifetime of a scope (visible in Nsight timelines; a
+// no-op without a tool attached)
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
 
 struct Arena {
     char* base = nullptr;
@@ -358,6 +367,7 @@ void parallel_sort(std::vector<T>& a, Less less) {
 }
 
 void number_edges(HostInst& H, const std::vector<int>& em, const std::vector<int>& oth) {
+    Range rg("f2m number edges");
     struct K { double c; int e, o; int v; int64_t s; };
     // slots with nbr > v, numbered per node, filled side by side
     std::vector<int64_t> first(H.V + 1, 0);
@@ -705,6 +715,7 @@ f2m_status launch_classes(f2m_ctx* ctx, DevCall& C, const f2m_params& prm) {
 }
 
 f2m_status run_device(f2m_ctx* ctx, DevCall& C, const f2m_params& prm, bool build_graph, bool solve) {
+    Range rg("f2m enqueue device stages");
     F2M_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
     F2M_CUDA(launch_prep(C.B, ctx->stream, &ctx->launches));
     F2M_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
@@ -811,6 +822,7 @@ f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, boo
 
 f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& prm, f2m_result& R,
                              std::mutex* mu = nullptr) {
+    Range rg("f2m complete instance");
     HostInst& H = R.H;
     const double vb = prm.error_B * prm.error_B_comb;
     HostCheck HC(H, vb);
@@ -1084,6 +1096,7 @@ static f2m_status complete_batch(f2m_ctx* ctx, DevCall& C, const f2m_params& prm
     for (int b = 0; b < C.pl.n_inst; ++b)
         if (status[b] == kNeedsHost) todo.push_back(b);
     if (todo.empty()) return F2M_OK;
+    Range rg("f2m host comb stage");
     const Batch& B = C.B;
     const int ni = C.pl.n_inst;
     std::vector<int32_t> Vn(ni);
@@ -1282,7 +1295,8 @@ namespace {
 // The single-instance path: rounding/de-duplication, kNN graph and, when
 // `solve`, the dual descent, comb stage and primal.
 f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels, int32_t n,
-                       int32_t top_k, const f2m_params* params, bool solve, f2m_result** out) {
+                       int32_t top_k, const f2m_params* params, bool solve, f2m_result** out,
+                       const double* F0 = nullptr, int32_t nF0 = 0) {
     *out = nullptr;
     const int64_t offs[2] = {0, n};
     f2m_status s = check_args(ctx, 1, offs, top_k, params);
@@ -1338,6 +1352,18 @@ f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int
     C.B.K_in = nullptr;
     F2M_CUDA(launch_graph(C.B, C.deg, C.scan, ctx->stream, &ctx->launches));
     F2M_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+    if (F0) {  // warm start: the potentials of the same nodes (node order of a result)
+        int32_t V = 0;
+        F2M_CUDA(cudaMemcpyAsync(&V, C.B.Vn, sizeof(V), cudaMemcpyDeviceToHost, ctx->stream));
+        F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (V != nF0)
+            return fail(ctx, F2M_ERR_INPUT, "the starting potentials have " + std::to_string(nF0) +
+                                                " values for " + std::to_string(V) + " nodes");
+        // the per-point "shift" buffer is free until a repair step: use it for F0
+        F2M_CUDA(cudaMemcpyAsync(const_cast<double*>(C.B.shift), F0, V * sizeof(double),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+        C.B.F0 = C.B.shift;
+    }
     if (!solve) {  // the graph only: edges in the reference's edge order
         F2M_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
         F2M_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1379,6 +1405,13 @@ extern "C" {
 f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels,
                             int32_t n, int32_t top_k, const f2m_params* params, f2m_result** out) {
     return points_call(ctx, x, y, labels, n, top_k, params, true, out);
+}
+
+f2m_status f2m_solve_points_from(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels,
+                                 int32_t n, int32_t top_k, const double* F0, int32_t n_F0,
+                                 const f2m_params* params, f2m_result** out) {
+    if (!F0) return ctx ? fail(ctx, F2M_ERR_INPUT, "F0 is required") : F2M_ERR_INPUT;
+    return points_call(ctx, x, y, labels, n, top_k, params, true, out, F0, n_F0);
 }
 
 f2m_status f2m_knn(f2m_ctx* ctx, const double* x, const double* y, const int32_t* labels, int32_t n,

@@ -136,6 +136,18 @@ typedef struct f2m_result f2m_result;
 f2m_status f2m_solve_points(f2m_ctx* ctx, const double* x, const double* y,
                             const int32_t* labels, int32_t n, int32_t top_k,
                             const f2m_params* params, f2m_result** out);
+/* Resume from stored potentials (no counterpart in the reference, which
+ * always starts from F = 0, graph_cuda_init.hpp:183): as f2m_solve_points,
+ * with the descent started from F0 (n_F0 values in the node order of a
+ * result for the same points and top_k, f2m_result_nodes) and run with the
+ * schedule the reference uses after a repair shift (run_fix,
+ * graph_cuda.cu:204-226: active-set rounds until max|grad| < error_B), so
+ * good potentials converge in far fewer iterations.  F2M_ERR_INPUT if n_F0
+ * is not the node count. */
+f2m_status f2m_solve_points_from(f2m_ctx* ctx, const double* x, const double* y,
+                                 const int32_t* labels, int32_t n, int32_t top_k,
+                                 const double* F0, int32_t n_F0, const f2m_params* params,
+                                 f2m_result** out);
 /* graph_c(graph*) + graph::RUN() (F2M.h:175,320) on a graph the caller
  * built: n_edges edges between node indices v1/v2 (either order) in the
  * reference's edge order (graph::E, ascending Do, graph_tour.hpp:28-98),

@@ -300,3 +300,54 @@ def test_solve_graph_matches_oracle(ctx, oracle):
             assert np.array_equal(r.x, o.x)
         p = ctx.solve_points(x, y, N)  # the same graph through the points path
         assert np.array_equal(p.F, r.F)
+
+
+# --- failures made on the host: caps, bad files, zero-length edges ----------
+
+def test_iteration_cap_reports_not_converged(ctx, oracle):
+    x, y = synth.uniform_int_points(400, 3)
+    p = f2m_b200.default_params(max_iters=50)
+    r = ctx.solve_points(x, y, 10, params=p)  # raises only for hard errors
+    assert r.status == f2m_b200.ERR_NOT_CONVERGED
+    lp, st = ctx.solve_batch(np.array([0, 400]), x, y, 10, params=p)
+    assert st[0] == f2m_b200.ERR_NOT_CONVERGED and np.isnan(lp[0])
+
+
+def test_malformed_files_are_input_errors(ctx, tmp_path):
+    bad = tmp_path / "bad.tsp"
+    bad.write_text("NAME : bad\nNODE_COORD_SECTION\n1 0 0\n2 x 7\nEOF\n")
+    with pytest.raises(f2m_b200.F2MError) as e:
+        ctx.solve_file(str(bad), 5)
+    assert e.value.status == f2m_b200.ERR_INPUT
+    empty = tmp_path / "empty.tsp"
+    empty.write_text("NAME : empty\nNODE_COORD_SECTION\nEOF\n")
+    with pytest.raises(f2m_b200.F2MError) as e:
+        ctx.solve_file(str(empty), 5)
+    assert e.value.status == f2m_b200.ERR_INPUT
+
+
+def test_zero_length_nint_edge_is_an_input_error(ctx, oracle):
+    """Two points 0.3 apart (distinct after the 1e-3 rounding) have nint cost 0."""
+    x, y = synth.uniform_int_points(60, 12)
+    x = np.concatenate([x, [x[0] + 0.3]])
+    y = np.concatenate([y, [y[0]]])
+    p = f2m_b200.default_params(cost_mode=1)
+    o = oracle.solve_points(x, y, 6, cost=oracle.COST_NINT)
+    assert o.status == oracle.ERR_INPUT
+    with pytest.raises(f2m_b200.F2MError) as e:
+        ctx.solve_points(x, y, 6, params=p)
+    assert e.value.status == f2m_b200.ERR_INPUT
+
+
+def test_resume_from_stored_potentials(ctx):
+    """Checkpoint/resume: the potentials of a result restart the descent; from
+    the optimum the same LP comes back in far fewer iterations."""
+    for (x, y), N in [(synth.uniform_int_points(1200, 81), 12), (synth.config2(3, n=15000), 16)]:
+        r1 = ctx.solve_points(x, y, N)
+        r2 = ctx.solve_points_from(x, y, N, r1.F)
+        assert r1.status == r2.status == 0
+        assert _close(r1.lp, r2.lp)
+        assert r2.stats["iterations"] < r1.stats["iterations"] / 2
+        with pytest.raises(f2m_b200.F2MError) as e:
+            ctx.solve_points_from(x, y, N, r1.F[:-1])
+        assert e.value.status == f2m_b200.ERR_INPUT
