@@ -150,13 +150,16 @@ __device__ __forceinline__ double red_d(const Slot& s, int v, HP H, double hv) {
     return (v < s.nbr) ? (s.D + hv) + hn : (s.D + hn) + hv;
 }
 
-// Sorted insertion of x into (v0 <= v1 <= v2) keeping the three smallest.
+// Sorted insertion of x into (v0 <= v1 <= v2) keeping the three smallest:
+// the reference's compare chain (strict <, so ties and NaN leave the triple
+// as it is) written as three compares and selects.  The selects run on the
+// integer pipe; the FP64 pipe, which bounds the dual step on this GPU, only
+// sees the compares.
 __device__ __forceinline__ void top3_insert(double x, double& v0, double& v1, double& v2) {
-    const double t = fmax(v0, x);
-    v0 = fmin(v0, x);
-    const double u = fmax(v1, t);
-    v1 = fmin(v1, t);
-    v2 = fmin(v2, u);
+    const bool c0 = x < v0, c1 = x < v1, c2 = x < v2;
+    v2 = c1 ? v1 : (c2 ? x : v2);
+    v1 = c0 ? v0 : (c1 ? x : v1);
+    v0 = c0 ? x : v0;
 }
 template <class HP>
 __device__ __forceinline__ double pdv(const Inst& I, int64_t r0, const uint16_t* list, int k, int v, HP H,

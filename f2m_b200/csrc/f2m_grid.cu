@@ -2,16 +2,28 @@
 //
 // The same schedule as the per-team solver (graph_cuda.cu:163-430 and the
 // comb stage, graph_cuda_comb.hpp:415-475), for instances whose potentials no
-// longer fit one SM's shared memory (10^5+ nodes).  Each CTA owns a
-// contiguous range of nodes; H = F/2 (double-buffered) and the comb labels
-// live in global memory and are read through L2 (ld.volatile) because other
-// SMs write them; a CTA's EF lists are cached in its shared memory.  A
-// bounded software grid barrier separates the Jacobi steps; the launch is
-// cooperative, so all CTAs are resident.  A barrier that waits too long sets
-// an error flag and every CTA returns.
+// longer fit one SM's shared memory (10^5+ nodes).  Each CTA owns a spatially
+// compact run of nodes (Morton order of the points); H = F/2 (double-buffered)
+// and the comb labels live in global memory and are read through L2
+// (ld.global.cg) because other SMs write them; a CTA's EF lists are cached in
+// its shared memory.  The launch is cooperative, so all CTAs are resident,
+// and a bounded software grid barrier orders the steps; a barrier that waits
+// too long sets an error flag and every CTA returns.
+//
+// Halo blocks.  Between two rebuilds of the active sets the Jacobi steps read
+// only the EF lists, so a CTA that holds the potentials of every node within
+// k EF hops of its own nodes (its halo, in shared memory) can run k steps
+// alone: step t recomputes the nodes within k-t hops, and after k steps its
+// own nodes hold exactly the values k global steps would give (every node's
+// update is the same function of the same inputs).  One grid barrier then
+// covers k steps instead of one.  k is the largest depth whose halo and EF
+// entries fit every CTA's shared memory (at most the block depth, 4 by
+// default); k = 0 falls back to one barrier per step.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include "f2m_device.cuh"
 #include "f2m_internal.h"
@@ -20,6 +32,9 @@ namespace f2m {
 
 constexpr int kGT = 1024;              // threads per CTA (one CTA per SM: fewer barrier arrivals)
 constexpr long long kSpinLimit = 1LL << 26;  // ~seconds of waiting before giving up
+constexpr int kMaxBlk = 16;            // most Jacobi steps between two grid barriers
+constexpr int kMaxNl = 2048;           // most nodes in a CTA's halo
+constexpr unsigned long long kHEmpty = ~0ull;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     unsigned v;
@@ -48,31 +63,218 @@ struct L2Ptr {
     __device__ __forceinline__ double operator[](int64_t i) const { return __ldcg(p + i); }
 };
 
+// grad/2 of one node from its EF list (cuda_get_Nodes_grad_R,
+// graph_cuda_grad.hpp): from the three smallest of the reduced costs and two
+// 1e6 sentinels.  Each word holds the neighbour's index into H and, in bit
+// 31, whether the neighbour is the lower node id (the order of the two
+// additions).  Entry k of a list is at Dp[k * ST], Wp[k * ST] (ST = 1:
+// contiguous lists; ST = 32: SELL-32 slices, entry k of 32 nodes side by
+// side).  The global and the halo steps both run this code, so their results
+// are identical.
+//
+// While the first reduced cost is below 1e6 (always, in practice) the
+// reference's compare chain is a sorted insertion (top3_insert); otherwise
+// the chain itself runs (it can then leave the triple unsorted).
+template <class HA>
+__device__ __forceinline__ double red_x(uint32_t w, double d, const HA& H, double hv) {
+    const double hw = H[w & 0x7fffffffu];
+    const bool first = (w >> 31) != 0;
+    return (d + (first ? hw : hv)) + (first ? hv : hw);
+}
+template <int ST, class HA>
+__device__ __forceinline__ double grad_chain(int n, const double* Dp, const uint32_t* Wp, const HA& H, double hv) {
+    double x0 = red_x(Wp[0], Dp[0], H, hv), x1 = 1e6, x2 = 1e6;
+    for (int k = 1; k < n; ++k) {
+        const double x = red_x(Wp[k * ST], Dp[k * ST], H, hv);
+        if (x < x0) { x2 = x1; x1 = x0; x0 = x; continue; }
+        if (x < x1) { x2 = x1; x1 = x; continue; }
+        if (x < x2) { x2 = x; }
+    }
+    return (-(x1 + x2) / 2) * 0.5;
+}
+template <int ST, class HA>
+__device__ __forceinline__ double grad_half(int n, const double* Dp, const uint32_t* Wp, const HA& H, double hv) {
+    if (n <= 0) return (-(1e6 + 1e6) / 2) * 0.5;
+    const double xf = red_x(Wp[0], Dp[0], H, hv);
+    if (!(xf < 1e6)) return grad_chain<ST>(n, Dp, Wp, H, hv);
+    double a0 = xf, a1 = 1e6, a2 = 1e6;
+    constexpr int CH = 4;  // entries loaded ahead of their insertions
+    for (int k0 = 1; k0 < n; k0 += CH) {
+        double x[CH];
+#pragma unroll
+        for (int j = 0; j < CH; ++j)
+            x[j] = (k0 + j < n) ? red_x(Wp[(k0 + j) * ST], Dp[(k0 + j) * ST], H, hv) : INFINITY;
+#pragma unroll
+        for (int j = 0; j < CH; ++j) top3_insert(x[j], a0, a1, a2);
+    }
+    return (-(a1 + a2) / 2) * 0.5;
+}
+
+// qpart_ptr_B / qpart_ptr_EF (graph_cuda_partition.hpp:3-54) for the grid
+// solver, where every reduced cost is a chain of three global loads (list
+// position, slot, neighbour potential through L2).  The scans evaluate kPf
+// positions ahead and then test them in order, so the loads of a chunk
+// overlap; the tests, the swaps, the threshold sequence and therefore the
+// final order and count are those of qpart_b / qpart_ef.
+constexpr int kPf = 8;
+__device__ __forceinline__ int qpart_b_g(const Inst& I, int64_t r0, int v, L2Ptr H, int size, double avg) {
+    uint16_t* list = I.perm + r0;
+    const double hv = H[v];
+    int low = 0, high = size - 1, i = low, j = high;
+    for (int pass = 0; i < j && pass <= size; ++pass) {
+        for (bool go = true; go;) {  // while (i <= high && pdv(i) <= avg) i++
+            double d[kPf];
+#pragma unroll
+            for (int c = 0; c < kPf; ++c) d[c] = (i + c <= high) ? pdv(I, r0, list, i + c, v, H, hv) : 0.0;
+#pragma unroll
+            for (int c = 0; c < kPf; ++c)
+                if (go) {
+                    if (i <= high && d[c] <= avg) ++i;
+                    else go = false;
+                }
+        }
+        for (bool go = true; go;) {  // while (j >= low && pdv(j) > avg) j--
+            double d[kPf];
+#pragma unroll
+            for (int c = 0; c < kPf; ++c) d[c] = (j - c >= low) ? pdv(I, r0, list, j - c, v, H, hv) : 0.0;
+#pragma unroll
+            for (int c = 0; c < kPf; ++c)
+                if (go) {
+                    if (j >= low && d[c] > avg) --j;
+                    else go = false;
+                }
+        }
+        if (i < j) { const uint16_t t = list[i]; list[i] = list[j]; list[j] = t; }
+    }
+    return j + 1;
+}
+__device__ __forceinline__ int qpart_ef_g(const Inst& I, int64_t r0, int v, L2Ptr H, int size, double avg,
+                                          int ef_min) {
+    if (size < ef_min) return size;
+    constexpr int kLimit = 1 << 20;
+    const uint16_t* list = I.perm + r0;
+    const double hv = H[v];
+    for (int bump = 0; bump < kLimit;) {
+        const int p = qpart_b_g(I, r0, v, H, size, avg);
+        if (p >= ef_min) return p;
+        double g = INFINITY;
+        bool nan = false;
+        for (int k0 = 0; k0 < size; k0 += kPf) {
+            double d[kPf];
+#pragma unroll
+            for (int c = 0; c < kPf; ++c) d[c] = (k0 + c < size) ? pdv(I, r0, list, k0 + c, v, H, hv) : 0.0;
+#pragma unroll
+            for (int c = 0; c < kPf; ++c)
+                if (k0 + c < size) {
+                    nan |= (d[c] != d[c]);
+                    if (k0 + c >= p) g = fmin(g, d[c]);
+                }
+        }
+        avg += 1;
+        ++bump;
+        if (nan) continue;
+        while (avg < g && bump < kLimit) {
+            avg += 1;
+            ++bump;
+        }
+    }
+    return size;
+}
+
+// Open-addressing table node -> local index in shared memory (the halo
+// build).  An entry is (node << 32 | local index); node ids are below 2^31,
+// so the all-ones word marks a free entry.
+__device__ __forceinline__ unsigned hslot(int key, unsigned mask) { return ((unsigned)key * 2654435761u) & mask; }
+
+// Inserts `key` if absent, numbering it with the next local index; returns
+// false when the table is full (the caller gives up the deeper levels).
+__device__ __forceinline__ bool h_insert(unsigned long long* ht, unsigned mask, int key, int* count, int* map,
+                                         int nl) {
+    volatile unsigned long long* vt = ht;
+    const unsigned long long tag = (unsigned long long)(unsigned)key << 32;
+    unsigned h = hslot(key, mask);
+    for (unsigned p = 0; p <= mask; ++p, h = (h + 1) & mask) {
+        unsigned long long cur = vt[h];
+        if (cur == kHEmpty) {
+            cur = atomicCAS(ht + h, kHEmpty, tag | 0xffffffffull);
+            if (cur == kHEmpty) {
+                const int idx = atomicAdd(count, 1);
+                if (idx < nl) map[idx] = key;
+                atomicExch(ht + h, tag | (unsigned)idx);
+                return true;
+            }
+        }
+        if ((cur >> 32) == (unsigned)key) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ int h_find(const unsigned long long* ht, unsigned mask, int key) {
+    unsigned h = hslot(key, mask);
+    for (unsigned p = 0; p <= mask; ++p, h = (h + 1) & mask) {
+        const unsigned long long cur = ht[h];
+        if (cur == kHEmpty) return -1;
+        if ((cur >> 32) == (unsigned)key) return (int)(unsigned)cur;
+    }
+    return -1;
+}
+// sets the local index of a key that is in the table
+__device__ __forceinline__ void h_set(unsigned long long* ht, unsigned mask, int key, int idx) {
+    unsigned h = hslot(key, mask);
+    for (unsigned p = 0; p <= mask; ++p, h = (h + 1) & mask)
+        if ((ht[h] >> 32) == (unsigned)key) {
+            ht[h] = ((unsigned long long)(unsigned)key << 32) | (unsigned)idx;
+            return;
+        }
+}
+
+// Shared-memory halo of one CTA.  Local nodes are numbered by EF-hop level:
+// [0, lend[0]) are the CTA's own nodes, [lend[d-1], lend[d]) those first
+// reached after d hops; inside a level, by decreasing list length.
+struct Halo {
+    double* h;             // [2*nl] potentials of the local nodes (two buffers); hash table while building
+    int* map;              // [nl] local index -> node
+    int* nn;               // [nl+1] EF list length of each computed node
+    double* D;             // [ne] EF entries in SELL-32 slices: reduced-cost base D
+    uint32_t* W;           // [ne] local neighbour index | lower-id flag
+    int* lend;             // shared [kMaxBlk+1]
+    int* cnt;              // shared [2]: inserted nodes, table-full flag
+    int* sb;               // shared [kMaxNl/32+1]: first entry of each 32-node slice
+    int* hist;             // shared [kGT]: counting-sort buckets (level, list length)
+    int nl = 0, ne = 0;
+    int kmax = 0;
+    int K = 0;             // steps per block of the current active sets (same on every CTA)
+    bool built = false;
+    long long own_slots = 0;  // EF entries of this thread's own nodes
+};
+
 struct GridSolver {
     const Batch& B;
     const DevParams& P;
     const GridState& G;
     const Inst& I;
     int b;
-    int v0, v1;            // this CTA's nodes
+    int o0, o1;            // this CTA's nodes: G.own[o0 .. o1)
     int64_t row0;          // first slot of the instance
     double* Hc;
     double* Hn;
-    double* eD;            // shared-memory EF cache of this CTA
+    double* eD;            // shared-memory EF cache of this CTA's own nodes
     uint32_t* eW;
     int cap;
-    int* sefo;             // shared: local offset of each own node's EF list (v1-v0+1)
+    int* sefo;             // shared: offset of each own node's EF list in the cache
     double* sred;
     long long* sredl;
     int* swarp;
     unsigned long long* sbcv;  // shared broadcast slot of the grid reductions
     int* sflag;                // shared: barrier error flag of this CTA
+    Halo L;
     int phase = 0;
     long long iters = 0, wslots = 0;
     int checks = 0;
     bool capped = false;
     bool dead = false;     // a barrier timed out
 
+    __device__ int nown() const { return o1 - o0; }
+    __device__ int node(int i) const { return G.own[o0 + i]; }  // i-th own node
     __device__ int deg(int v) const { return (int)(I.row[v + 1] - I.row[v]); }
 
     // Bounded grid barrier (arrival count + generation).  Thread 0 of each CTA
@@ -147,60 +349,25 @@ struct GridSolver {
 
     __device__ __forceinline__ L2Ptr hc() const { return L2Ptr{Hc}; }
 
-    // grad/2 of an own node over its EF list (the first efcnt slots of its
-    // list, held in shared memory or in the slot-indexed arena).  The
-    // neighbours' potentials come from L2; they are loaded four at a time
-    // ahead of the compare chain, so one L2 latency covers four entries.
-    __device__ double hgrad(int v) const {
+    // grad/2 of the i-th own node over its EF list (the first efcnt slots of
+    // its list, held in shared memory or in the slot-indexed arena)
+    __device__ double hgrad(int i, int v) const {
         const int n = G.efc[v];
-        const int lo = sefo[v - v0];
+        const int lo = sefo[i];
         const bool sm = lo + n <= cap;
         const int64_t go = I.row[v] - row0;
         const double* Dp = sm ? eD + lo : G.gD + go;
         const uint32_t* Wp = sm ? eW + lo : G.gW + go;
         const L2Ptr H = hc();
-        const double hv = H[v];
-        constexpr int CH = 4;
-        double x0 = 0.0, x1 = 1e6, x2 = 1e6;
-        bool chain = false;
-        for (int k0 = 0; k0 < n; k0 += CH) {
-            double hw[CH], dd[CH];
-            uint32_t ww[CH];
-#pragma unroll
-            for (int j = 0; j < CH; ++j) {
-                ww[j] = 0u;
-                hw[j] = 0.0;
-                dd[j] = 0.0;
-                if (k0 + j < n) {
-                    ww[j] = Wp[k0 + j];
-                    dd[j] = Dp[k0 + j];
-                    hw[j] = H[ww[j] & 0x7fffffffu];
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < CH; ++j) {
-                if (k0 + j >= n) break;
-                const bool first = (ww[j] >> 31) != 0;
-                const double x = (dd[j] + (first ? hw[j] : hv)) + (first ? hv : hw[j]);
-                if (k0 + j == 0) {  // cuda_get_Nodes_grad_R: chain unless the first is below 1e6
-                    x0 = x;
-                    chain = !(x0 < 1e6);
-                } else if (!chain) {
-                    top3_insert(x, x0, x1, x2);
-                } else {
-                    if (x < x0) { x2 = x1; x1 = x0; x0 = x; continue; }
-                    if (x < x1) { x2 = x1; x1 = x; continue; }
-                    if (x < x2) { x2 = x; }
-                }
-            }
-        }
-        return (-(x1 + x2) / 2) * 0.5;
+        return grad_half<1>(n, Dp, Wp, H, H[v]);
     }
     __device__ void swap_h() { double* t = Hc; Hc = Hn; Hn = t; }
+    // one global Jacobi step (one grid barrier)
     template <bool MASKED>
     __device__ void step() {
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
-            const double g = hgrad(v);
+        for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
+            const double g = hgrad(i, v);
             const double h = hc()[v];
             Hn[v] = (MASKED && B.shift[I.base + v] != 0.0) ? h : h + g;
             wslots += G.efc[v];  // this thread's active slots
@@ -211,26 +378,31 @@ struct GridSolver {
     }
     __device__ double grad_max() {
         double m = 0.0;
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) m = fmax(m, fabs(hgrad(v)));
+        for (int i = threadIdx.x; i < nown(); i += kGT) m = fmax(m, fabs(hgrad(i, node(i))));
         return 2.0 * gmax(m);
+    }
+    // EF-list offsets of the own nodes in the shared cache
+    __device__ void own_offsets() {
+        __syncthreads();
+        int carry = 0;
+        for (int r = 0; r < nown(); r += kGT) {
+            const int i = r + threadIdx.x;
+            const int c = (i < nown()) ? G.efc[node(i)] : 0;
+            int tot;
+            const int ex = block_excl_scan<kGT>(c, swarp, &tot);
+            if (i < nown()) sefo[i] = carry + ex;
+            carry += tot;
+        }
+        if (threadIdx.x == 0) sefo[nown()] = carry;
+        __syncthreads();
     }
     // update_EF for this CTA's nodes: local offsets, shared cache, arena copy
     __device__ void rebuild_ef() {
-        __syncthreads();
-        int carry = 0;
-        for (int r = v0; r < v1; r += kGT) {
-            const int v = r + threadIdx.x;
-            const int c = (v < v1) ? G.efc[v] : 0;
-            int tot;
-            const int ex = block_excl_scan<kGT>(c, swarp, &tot);
-            if (v < v1) sefo[v - v0] = carry + ex;
-            carry += tot;
-        }
-        if (threadIdx.x == 0) sefo[v1 - v0] = carry;
-        __syncthreads();
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
+        own_offsets();
+        for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
             const int64_t r0 = I.row[v];
-            const int n = G.efc[v], lo = sefo[v - v0];
+            const int n = G.efc[v], lo = sefo[i];
             const int64_t go = r0 - row0;
             const bool sm = lo + n <= cap;
             for (int k = 0; k < n; ++k) {
@@ -242,40 +414,206 @@ struct GridSolver {
             }
         }
         __syncthreads();
+        L.built = false;
     }
+
+    // Halo of the current EF lists: levels by EF hops from the own nodes,
+    // then the deepest k (<= kmax) whose nodes and entries fit, agreed over
+    // the grid (the minimum), then the entries of the nodes the steps
+    // recompute with their neighbours renumbered to local indices.  Other
+    // CTAs' lists and counts are read through L2 (ld.global.cg).
+    __device__ void build_halo() {
+        L.built = true;
+        L.K = 0;
+        if (L.nl == 0) return;
+        sync();  // every CTA's efc and arena lists are complete
+        if (dead) return;
+        unsigned long long* ht = reinterpret_cast<unsigned long long*>(L.h);
+        const unsigned mask = 2u * (unsigned)L.nl - 1u;
+        for (unsigned h = threadIdx.x; h <= mask; h += kGT) ht[h] = kHEmpty;
+        if (threadIdx.x == 0) { L.cnt[0] = 0; L.cnt[1] = 0; }
+        __syncthreads();
+        int depth = -1;
+        if (nown() <= L.nl) {
+            for (int i = threadIdx.x; i < nown(); i += kGT)
+                if (!h_insert(ht, mask, node(i), L.cnt, L.map, L.nl)) L.cnt[1] = 1;
+            __syncthreads();
+            if (!L.cnt[1]) {
+                L.lend[0] = nown();
+                depth = 0;
+            }
+            __syncthreads();
+            for (int d = 1; d <= L.kmax && depth == d - 1; ++d) {
+                const int f0 = d == 1 ? 0 : L.lend[d - 2], f1 = L.lend[d - 1];
+                for (int i = f0 + threadIdx.x; i < f1; i += kGT) {
+                    const int u = L.map[i];
+                    const int n = __ldcg(G.efc + u);
+                    const int64_t go = I.row[u] - row0;
+                    for (int k = 0; k < n; ++k)
+                        if (!h_insert(ht, mask, (int)(__ldcg(G.gW + go + k) & 0x7fffffffu), L.cnt, L.map, L.nl))
+                            L.cnt[1] = 1;
+                }
+                __syncthreads();
+                const int c = L.cnt[0], full = L.cnt[1];
+                if (!full && c <= L.nl) {
+                    if (threadIdx.x == 0) L.lend[d] = c;
+                    depth = d;
+                }
+                __syncthreads();
+            }
+        }
+        // The nodes of levels < depth (the ones a block may recompute) are
+        // renumbered level by level in decreasing list length, so the
+        // 32-node slices of the SELL layout carry little padding; a counting
+        // sort over (level, 63 - min(length, 63)) keeps the levels in order.
+        int kc = 0;
+        if (depth >= 1) {
+            const int nc = L.lend[depth - 1];  // <= nl
+            L.hist[threadIdx.x] = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < nc; i += kGT) {  // bucket and rank, staged in nn
+                const int n = __ldcg(G.efc + L.map[i]);
+                int lvl = 0;
+                while (i >= L.lend[lvl]) ++lvl;
+                const int key = lvl * 64 + 63 - min(n, 63);
+                L.nn[i] = (key << 16) | atomicAdd(L.hist + key, 1);
+            }
+            __syncthreads();
+            {
+                int tot;
+                const int ex = block_excl_scan<kGT>(L.hist[threadIdx.x], swarp, &tot);
+                __syncthreads();
+                L.hist[threadIdx.x] = ex;
+            }
+            __syncthreads();
+            int* order = reinterpret_cast<int*>(L.D);  // the new order, staged in the entry array
+            for (int i = threadIdx.x; i < nc; i += kGT) {
+                const int kr = L.nn[i];
+                order[L.hist[kr >> 16] + (kr & 0xffff)] = L.map[i];
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < nc; i += kGT) {
+                const int u = order[i];
+                L.map[i] = u;
+                h_set(ht, mask, u, i);
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < nc; i += kGT) L.nn[i] = __ldcg(G.efc + L.map[i]);
+            __syncthreads();
+            // slice widths (warp-wide max) and their prefix
+            const int ns = (nc + 31) / 32;
+            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+            for (int sl = wid; sl < ns; sl += kGT / 32) {
+                const int i = sl * 32 + lane;
+                const int wdt = __reduce_max_sync(0xffffffffu, i < nc ? L.nn[i] : 0);
+                if (lane == 0) L.sb[sl + 1] = wdt * 32;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                L.sb[0] = 0;
+                for (int sl = 1; sl <= ns; ++sl) L.sb[sl] += L.sb[sl - 1];
+            }
+            __syncthreads();
+            for (int k = depth; k >= 1; --k)
+                if (L.sb[(L.lend[k - 1] + 31) / 32] <= L.ne) { kc = k; break; }
+        }
+        // the entries of levels < kc, neighbours renumbered to local indices:
+        // entry k of node i at sb[i/32] + 32 k + i%32
+        if (threadIdx.x == 0) L.cnt[1] = 0;
+        __syncthreads();
+        if (kc >= 1) {
+            const int nc = L.lend[kc - 1];
+            for (int i = threadIdx.x; i < nc; i += kGT) {
+                const int u = L.map[i];
+                const int n = L.nn[i];
+                const int64_t go = I.row[u] - row0;
+                const int base = L.sb[i >> 5] + (i & 31);
+                for (int k = 0; k < n; ++k) {
+                    const uint32_t w = __ldcg(G.gW + go + k);
+                    const int li = h_find(ht, mask, (int)(w & 0x7fffffffu));
+                    if (li < 0 || li >= L.lend[kc]) L.cnt[1] = 1;  // cannot happen: all within kc hops
+                    L.D[base + 32 * k] = __ldcg(G.gD + go + k);
+                    L.W[base + 32 * k] = (uint32_t)(li < 0 ? 0 : li) | (w & 0x80000000u);
+                }
+            }
+        }
+        __syncthreads();
+        if (L.cnt[1]) kc = 0;
+        L.own_slots = 0;
+        for (int i = threadIdx.x; i < nown(); i += kGT) L.own_slots += G.efc[node(i)];
+        L.K = (int)(-gmax_ll(-(long long)kc));
+        __syncthreads();
+    }
+
+    // n unmasked Jacobi steps: blocks of K halo steps with one grid barrier
+    // each, or single global steps when no halo fits
+    __device__ void steps(int n) {
+        if (!L.built) build_halo();
+        if (L.K == 0) {
+            for (int it = 0; it < n && !dead; ++it) step<false>();
+            return;
+        }
+        double* A = L.h;
+        double* Bn = L.h + L.nl;
+        for (int done = 0; done < n && !dead;) {
+            const int k = min(L.K, n - done);
+            const L2Ptr H = hc();
+            for (int i = threadIdx.x; i < L.lend[k]; i += kGT) A[i] = H[L.map[i]];
+            __syncthreads();
+            for (int t = 1; t <= k; ++t) {
+                const int m = L.lend[k - t];  // nodes within k-t hops
+                for (int i = threadIdx.x; i < m; i += kGT) {
+                    const int lo = L.sb[i >> 5] + (i & 31);
+                    const double h = A[i];
+                    Bn[i] = h + grad_half<32>(L.nn[i], L.D + lo, L.W + lo, A, h);
+                }
+                __syncthreads();
+                double* t2 = A;
+                A = Bn;
+                Bn = t2;
+            }
+            for (int i = threadIdx.x; i < nown(); i += kGT) Hn[L.map[i]] = A[i];
+            wslots += (long long)k * L.own_slots;
+            iters += k;
+            done += k;
+            sync();
+            swap_h();
+        }
+    }
+
     __device__ double check_opt() {
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
+        for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
             const int d = deg(v);
-            G.efc[v] = (d < P.ef_small_deg) ? d : qpart_ef(I, I.row[v], v, hc(), d, P.ef_thr, P.ef_min);
+            G.efc[v] = (d < P.ef_small_deg) ? d : qpart_ef_g(I, I.row[v], v, hc(), d, P.ef_thr, P.ef_min);
         }
         rebuild_ef();
         checks++;
         return grad_max();
     }
     __device__ void block_ef(int N) {
+        // cuda_block_EF: N steps, or check_every when the gradient at entry is
+        // already below error_B (the count check breaks there)
         const double MA = grad_max();
-        int count_M = 0;
-        for (int it = 0; it < N && !dead; ++it) {
-            step<false>();
-            if (++count_M >= P.check_every) {
-                if (MA < P.error_B) break;
-                count_M = 0;
-            }
-        }
+        steps(MA < P.error_B ? min(N, P.check_every) : N);
     }
     __device__ void block_glob() {
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) G.efc[v] = min(deg(v), P.glob_K);
+        for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
+            G.efc[v] = min(deg(v), P.glob_K);
+        }
         rebuild_ef();
         for (int go = 0; go < P.glob_rounds && !dead; ++go) {
-            for (int it = 0; it < P.glob_inner && !dead; ++it) step<false>();
-            for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
+            steps(P.glob_inner);
+            for (int i = threadIdx.x; i < nown(); i += kGT) {
+                const int v = node(i);
                 const int d = deg(v);
                 if (d < P.glob_K) { G.efc[v] = d; continue; }
                 const int64_t r0 = I.row[v];
                 const double hv = hc()[v];
                 double avg = pdv(I, r0, I.perm + r0, 0, v, hc(), hv);
                 for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, I.perm + r0, k, v, hc(), hv));
-                G.efc[v] = qpart_ef(I, r0, v, hc(), d, avg, P.ef_min);
+                G.efc[v] = qpart_ef_g(I, r0, v, hc(), d, avg, P.ef_min);
             }
             rebuild_ef();
             if (grad_max() < P.glob_tol) break;
@@ -309,9 +647,12 @@ struct GridSolver {
         const double porog = P.porog;
         int* ccnt = G.scratch;
         int* lab = G.scratch + V;
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT)  // cuda_partition_v3
-            ccnt[v] = qpart_b(I, I.row[v], v, hc(), G.efc[v], P.comb_thr);
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
+        for (int i = threadIdx.x; i < nown(); i += kGT) {  // cuda_partition_v3
+            const int v = node(i);
+            ccnt[v] = qpart_b_g(I, I.row[v], v, hc(), G.efc[v], P.comb_thr);
+        }
+        for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
             const int64_t r0 = I.row[v];
             const double hv = hc()[v];
             bool has = false;
@@ -327,7 +668,8 @@ struct GridSolver {
         volatile int* vlab = lab;
         for (int round = 0; round < V + 1 && !dead; ++round) {
             long long changed = 0;
-            for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
+            for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
                 int m = vlab[v];
                 if (m == INT_MAX) continue;
                 const int64_t r0 = I.row[v];
@@ -341,13 +683,15 @@ struct GridSolver {
             }
             if (gsum_ll(changed) == 0) break;
         }
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
+        for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
             B.F[I.base + v] = 2.0 * hc()[v];
             B.efcnt[I.base + v] = G.efc[v];
             B.ccnt[I.base + v] = ccnt[v];
         }
         volatile int* virr = G.irr;
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
+        for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
             const int l = vlab[v];
             if (l == INT_MAX) continue;
             const int64_t r0 = I.row[v], r1 = I.row[v + 1];
@@ -361,13 +705,16 @@ struct GridSolver {
         }
         sync();
         long long nc = 0, ni = 0;
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT)
+        for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
             if (vlab[v] == v) { nc++; ni += virr[v]; }
+        }
         nc = gsum_ll(nc);
         ni = gsum_ll(ni);
         double lp = 0.0, dual_neg = 0.0, fsum = 0.0;
         long long maxr = -1, viol = 0;
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
+        for (int i = threadIdx.x; i < nown(); i += kGT) {
+            const int v = node(i);
             const int64_t r0 = I.row[v], r1 = I.row[v + 1];
             const double hv = hc()[v];
             fsum += 2.0 * hv;
@@ -415,50 +762,69 @@ struct GridSolver {
     }
 };
 
+
 __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, GridState G, int b, int refit,
-                                                     int cap) {
+                                                     int cap, int nl, int ne, int kmax) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sred[kGT / 32];
     __shared__ long long sredl[kGT / 32];
     __shared__ int swarp[kGT / 32 + 1];
     __shared__ unsigned long long sbc[1];
     __shared__ int sflag[1];
+    __shared__ int slend[kMaxBlk + 1];
+    __shared__ int scnt[2];
+    __shared__ int ssb[kMaxNl / 32 + 1];
+    __shared__ int shist[kGT];
     const Inst I = make_inst(B, b);
     const int V = I.V;
-    const int v0 = (int)(((long long)V * blockIdx.x) / gridDim.x);
-    const int v1 = (int)(((long long)V * (blockIdx.x + 1)) / gridDim.x);
-    const int nv = v1 - v0;
+    const int o0 = (int)(((long long)V * blockIdx.x) / gridDim.x);
+    const int o1 = (int)(((long long)V * (blockIdx.x + 1)) / gridDim.x);
+    const int nv = o1 - o0;
+    // shared layout: own offsets | own EF cache (cap) | halo potentials (2 nl)
+    // | halo map (nl) | halo list lengths (nl+1) | halo entries (ne)
     int* sefo = reinterpret_cast<int*>(smem_raw);
-    const size_t head = (((size_t)nv + 1) * 4 + 15) / 16 * 16;
-    double* eD = reinterpret_cast<double*>(smem_raw + head);
-    uint32_t* eW = reinterpret_cast<uint32_t*>(eD + cap);
-    GridSolver S{B, P, G, I, b, v0, v1, I.row[0], G.Ha, G.Hb, eD, eW, cap, sefo, sred, sredl, swarp, sbc, sflag};
+    size_t off = (((size_t)nv + 1) * 4 + 15) / 16 * 16;
+    double* eD = reinterpret_cast<double*>(smem_raw + off);
+    off += (size_t)cap * 8;
+    uint32_t* eW = reinterpret_cast<uint32_t*>(smem_raw + off);
+    off += ((size_t)cap * 4 + 15) / 16 * 16;
+    GridSolver S{B, P, G, I, b, o0, o1, I.row[0], G.Ha, G.Hb, eD, eW, cap, sefo, sred, sredl, swarp, sbc, sflag};
+    S.L.h = reinterpret_cast<double*>(smem_raw + off);
+    off += (size_t)nl * 16;
+    S.L.map = reinterpret_cast<int*>(smem_raw + off);
+    off += (size_t)nl * 4;
+    S.L.nn = reinterpret_cast<int*>(smem_raw + off);
+    off += (((size_t)nl + 1) * 4 + 15) / 16 * 16;
+    S.L.D = reinterpret_cast<double*>(smem_raw + off);
+    off += (size_t)ne * 8;
+    S.L.W = reinterpret_cast<uint32_t*>(smem_raw + off);
+    S.L.lend = slend;
+    S.L.cnt = scnt;
+    S.L.sb = ssb;
+    S.L.hist = shist;
+    S.L.nl = nl;
+    S.L.ne = ne;
+    S.L.kmax = min(kmax, kMaxBlk);
     double M;
     if (!refit) {
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) G.Ha[v] = B.F0 ? 0.5 * B.F0[I.base + v] : 0.0;  // F = 0 or warm
+        for (int i = threadIdx.x; i < nv; i += kGT) {
+            const int v = S.node(i);
+            G.Ha[v] = B.F0 ? 0.5 * B.F0[I.base + v] : 0.0;  // F = 0 or warm
+        }
         S.sync();
         M = B.F0 ? S.run_fix() : S.run_start();  // a resumed descent skips the global phase
     } else {
         // cuda_IRREGULAR_B_recompute (graph_cuda_comb.hpp:542-574)
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
+        for (int i = threadIdx.x; i < nv; i += kGT) {
+            const int v = S.node(i);
             G.Ha[v] = 0.5 * (B.F[I.base + v] + B.shift[I.base + v]);
             G.efc[v] = B.efcnt[I.base + v];
         }
         // the EF lists of the last update_EF are in the slot-indexed arena
-        __syncthreads();
-        int carry = 0;
-        for (int r = v0; r < v1; r += kGT) {
-            const int v = r + threadIdx.x;
-            const int c = (v < v1) ? G.efc[v] : 0;
-            int tot;
-            const int ex = block_excl_scan<kGT>(c, swarp, &tot);
-            if (v < v1) sefo[v - v0] = carry + ex;
-            carry += tot;
-        }
-        if (threadIdx.x == 0) sefo[nv] = carry;
-        __syncthreads();
-        for (int v = v0 + threadIdx.x; v < v1; v += kGT) {
-            const int n = G.efc[v], lo = sefo[v - v0];
+        S.own_offsets();
+        for (int i = threadIdx.x; i < nv; i += kGT) {
+            const int v = S.node(i);
+            const int n = G.efc[v], lo = sefo[i];
             const int64_t go = I.row[v] - I.row[0];
             if (lo + n <= cap)
                 for (int k = 0; k < n; ++k) { eD[lo + k] = G.gD[go + k]; eW[lo + k] = G.gW[go + k]; }
@@ -470,19 +836,49 @@ __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, Gri
     S.combs_and_primal(M, refit != 0);
 }
 
-static size_t grid_smem_bytes(int32_t V, int grid, int* cap) {
+// Shared memory of one CTA: own-node offsets, the own EF cache (3 entries per
+// node; longer lists are read from the arena), and the halo (nl local nodes
+// at 24 B, the rest of the opt-in limit as 12-B entries).  nl is the power of
+// two >= 3x the own nodes, 1,024-2,048; CTAs with more than 2,048 own nodes
+// get no halo and step with one barrier per step.
+static size_t grid_smem_bytes(int32_t V, int grid, int* cap, int* nl, int* ne) {
     const int nv = (V + grid - 1) / grid + 1;
-    const size_t head = (((size_t)nv + 1) * 4 + 15) / 16 * 16;
-    // EF lists of a CTA's nodes: about 4 per node in the active phase, 5 in
-    // the first phase; lists beyond the cache are read from the arena
+    size_t off = (((size_t)nv + 1) * 4 + 15) / 16 * 16;
     int dev = 0, lim = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const long long room = ((long long)lim - 4096 - (long long)head) / 12;
-    long long c = (long long)nv * 8;
-    if (c > room) c = room > 0 ? room : 0;
+    const long long room = (long long)lim - 8192;  // static shared memory and alignment
+    int l = 1024;
+    while (l < 3 * nv && l < kMaxNl) l *= 2;
+    if (nv > kMaxNl) l = 0;
+    long long c = l ? (long long)nv * 3 : (room - (long long)off) / 12;
+    const long long halo_nodes = l ? (long long)l * 24 + 16 : 0;
+    long long e = l ? (room - (long long)off - c * 12 - 16 - halo_nodes) / 12 : 0;
+    if (l && e < 4LL * l) {  // not enough room for a useful halo
+        l = 0;
+        e = 0;
+        c = (room - (long long)off) / 12;
+    }
+    if (c < 0) c = 0;
     *cap = (int)c;
-    return head + (size_t)c * 12;
+    *nl = l;
+    *ne = (int)e;
+    off += (size_t)c * 8 + ((size_t)c * 4 + 15) / 16 * 16;
+    if (l) off += (size_t)l * 16 + (size_t)l * 4 + (((size_t)l + 1) * 4 + 15) / 16 * 16 + (size_t)e * 12;
+    return off;
+}
+
+// Jacobi steps per grid barrier at most (F2M_GRID_BLOCK overrides; 0 = one
+// barrier per step).  Deeper blocks recompute more halo nodes per step.
+static int grid_block_steps() {
+    static int k = -1;
+    if (k < 0) {
+        const char* e = getenv("F2M_GRID_BLOCK");
+        k = e ? atoi(e) : 4;
+        if (k < 0) k = 0;
+        if (k > kMaxBlk) k = kMaxBlk;
+    }
+    return k;
 }
 
 cudaError_t launch_solve_grid(const Batch& B, const DevParams& P, const GridState& G, int b, int V,
@@ -491,8 +887,8 @@ cudaError_t launch_solve_grid(const Batch& B, const DevParams& P, const GridStat
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int grid = sms;
-    int cap = 0;
-    size_t smem = grid_smem_bytes(V, grid, &cap);
+    int cap = 0, nl = 0, ne = 0;
+    size_t smem = grid_smem_bytes(V, grid, &cap, &nl, &ne);
     cudaError_t e = cudaFuncSetAttribute(k_solve_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -501,18 +897,82 @@ cudaError_t launch_solve_grid(const Batch& B, const DevParams& P, const GridStat
     if (per_sm > 2) per_sm = 2;
     grid = sms * per_sm;
     if (grid > kGridMaxCtas) grid = kGridMaxCtas;
-    smem = grid_smem_bytes(V, grid, &cap);
+    smem = grid_smem_bytes(V, grid, &cap, &nl, &ne);
     if ((e = cudaMemsetAsync(G.bar, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(G.err, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
     Batch Bc = B;
     DevParams Pc = P;
     GridState Gc = G;
-    int bb = b, rf = refit ? 1 : 0, cp = cap;
-    void* args[] = {&Bc, &Pc, &Gc, &bb, &rf, &cp};
+    int bb = b, rf = refit ? 1 : 0, cp = cap, l = nl, en = ne, km = grid_block_steps();
+    if (km == 0) l = 0;
+    void* args[] = {&Bc, &Pc, &Gc, &bb, &rf, &cp, &l, &en, &km};
     e = cudaLaunchCooperativeKernel((const void*)k_solve_grid, dim3(grid), dim3(kGT), args, smem, s);
     ++*launches;
     return e;
 }
 
+/* ------------------------------------------------------------------ */
+/* ownership order: Morton order of the points                          */
+/* ------------------------------------------------------------------ */
+__device__ __forceinline__ unsigned spread16(unsigned v) {
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+// key = Morton code of the point on a 2^16 x 2^16 lattice over the square
+// that holds the instance's cell grid, then the node id (ties, and the
+// order itself when spatial == 0).  n >= the instance's node count; the
+// entries past it take the largest code and sort last.
+__global__ void k_own_keys(Batch B, int b, int n, const int32_t* point_of, int spatial, unsigned long long* key) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    unsigned m = 0;
+    if (v >= B.Vn[b]) {
+        m = 0xffffffffu;
+    } else if (spatial) {
+        const int p = point_of ? point_of[v] : v;
+        const double2 q = B.P[B.offs[b] + p];
+        const double w = B.gh[b] * (double)max(B.gnx[b], B.gny[b]);
+        const double fx = fmin(fmax((q.x - B.gx0[b]) / w, 0.0), 1.0) * 65535.0;
+        const double fy = fmin(fmax((q.y - B.gy0[b]) / w, 0.0), 1.0) * 65535.0;
+        m = spread16((unsigned)fx) | (spread16((unsigned)fy) << 1);
+    }
+    key[v] = ((unsigned long long)m << 32) | (unsigned)v;
+}
+__global__ void k_own_take(const unsigned long long* key, int n, int32_t* own) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) own[i] = (int32_t)(unsigned)key[i];
+}
+
+size_t grid_order_temp_bytes(int64_t n) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                   (int)n, 32, 64);
+    return bytes;
+}
+
+cudaError_t launch_grid_order(const Batch& B, const GridState& G, int b, int V, const int32_t* point_of,
+                              bool spatial, cudaStream_t s, int64_t* launches) {
+    if (V <= 0) return cudaSuccess;
+    const int T = 256, nb = (V + T - 1) / T;
+    k_own_keys<<<nb, T, 0, s>>>(B, b, V, point_of, spatial ? 1 : 0, G.okey);
+    ++*launches;
+    const unsigned long long* sorted = G.okey;
+    if (spatial) {
+        // the sort is stable, so equal codes keep the node order
+        size_t bytes = G.otmp_bytes;
+        cudaError_t e = cub::DeviceRadixSort::SortKeys(G.otmp, bytes, G.okey, G.okey2, V, 32, 64, s);
+        if (e != cudaSuccess) return e;
+        ++*launches;
+        sorted = G.okey2;
+    }
+    k_own_take<<<nb, T, 0, s>>>(sorted, V, G.own);
+    ++*launches;
+    return cudaGetLastError();
+}
 
 }  // namespace f2m

@@ -135,12 +135,23 @@ struct GridState {
     int32_t* err;           // [1] set when a barrier timed out
     double* part;           // [2*grid] partial reductions
     long long* partl;       // [2*grid]
+    int32_t* own;           // [V] nodes in ownership order (CTA c owns a contiguous run)
+    unsigned long long* okey;   // [V] ownership sort keys (Morton code << 32 | node)
+    unsigned long long* okey2;  // [V]
+    void* otmp;             // radix-sort scratch
+    size_t otmp_bytes;
 };
 constexpr int kGridMaxCtas = 2 * 160;
 
 // Host-side launchers (f2m_kernels.cu, f2m_grid.cu).
 cudaError_t launch_solve_grid(const Batch& B, const DevParams& P, const GridState& G, int b, int V,
                               bool refit, cudaStream_t s, int64_t* launches);
+// Ownership order of the grid solver's nodes: Morton order of the points
+// (point_of[v] = point of node v, or nullptr when node = point), or the node
+// order itself when the instance has no coordinates (spatial = false).
+cudaError_t launch_grid_order(const Batch& B, const GridState& G, int b, int V, const int32_t* point_of,
+                              bool spatial, cudaStream_t s, int64_t* launches);
+size_t grid_order_temp_bytes(int64_t n);
 cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches);
 cudaError_t launch_knn(const Batch& B, int64_t* scan_scratch, cudaStream_t s, int64_t* launches);
 cudaError_t launch_graph(const Batch& B, int64_t* deg_scratch, int64_t* scan_scratch,

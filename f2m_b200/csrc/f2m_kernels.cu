@@ -852,7 +852,7 @@ __device__ __forceinline__ double ef_d(double D, uint16_t w, double hv, const do
 // cuda_get_Nodes_grad_R (graph_cuda_grad.hpp:321-340): grad = -(v1+v2)/2 over
 // the 2nd and 3rd smallest of {first, rest.., 1e6, 1e6}.  While the first value
 // is below 1e6 the reference's compare chain keeps v0<=v1<=v2 and is a sorted
-// insertion (top3_insert, a branch-free min/max network); otherwise the chain
+// insertion (top3_insert, branch-free compares and selects); otherwise the chain
 // itself runs (it can then leave v0 > v1).  Returns grad/2, the step of H.
 template <class Get>
 __device__ __forceinline__ double half_grad(int n, Get get) {

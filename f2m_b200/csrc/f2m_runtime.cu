@@ -209,6 +209,11 @@ void carve_grid(Arena& A, GridState& G, int64_t n, int64_t S) {
     G.err = A.take<int32_t>(4);
     G.part = A.take<double>(2 * kGridMaxCtas);
     G.partl = A.take<long long>(2 * kGridMaxCtas);
+    G.own = A.take<int32_t>(n);
+    G.okey = A.take<unsigned long long>(n);
+    G.okey2 = A.take<unsigned long long>(n);
+    G.otmp_bytes = grid_order_temp_bytes(n);
+    G.otmp = A.take<unsigned char>(G.otmp_bytes);
 }
 
 void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, int64_t** scan_scratch,
@@ -655,6 +660,7 @@ struct DevCall {
     Batch B{};
     GridState G{};
     bool grid = false;      // the single large instance runs on the grid-wide solver
+    bool spatial = true;    // the grid solver's nodes can be ordered by their points (node = point)
     int64_t* deg = nullptr;
     int64_t* scan = nullptr;
     int32_t *ci = nullptr, *cs = nullptr, *ord = nullptr;
@@ -697,6 +703,7 @@ f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h
 f2m_status launch_classes(f2m_ctx* ctx, DevCall& C, const f2m_params& prm) {
     const DevParams P = to_dev(prm);
     if (C.grid) {
+        F2M_CUDA(launch_grid_order(C.B, C.G, 0, C.pl.max_n, nullptr, C.spatial, ctx->stream, &ctx->launches));
         F2M_CUDA(launch_solve_grid(C.B, P, C.G, 0, C.pl.max_n, false, ctx->stream, &ctx->launches));
         return F2M_OK;
     }
@@ -1494,6 +1501,7 @@ f2m_status f2m_solve_graph(f2m_ctx* ctx, int32_t n_nodes, int32_t n_edges, const
     f2m_status st = setup_call(ctx, C, 1, offs, cap_n, prm, true);
     if (st) return st;
     if (C.B.S_cap < S) return fail(ctx, F2M_ERR_CAPACITY, "graph too dense for the solver's list arrays");
+    C.spatial = false;  // no coordinates: the grid solver keeps the caller's node order
     Batch& B = C.B;
     std::vector<int32_t> mirror32(H.mirror.begin(), H.mirror.end());
     const int32_t one_v = n_nodes, ok = F2M_OK;
@@ -1989,6 +1997,11 @@ f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k, const f
     // graph::RUN (graph_cuda.cu:47-155), timed like dtimeRUN
     auto t0 = std::chrono::steady_clock::now();
     if (C.grid) {
+        // nodes in the reference's order, points in file order: order the
+        // nodes by their points (fxy_of, staged in the ownership buffer)
+        std::vector<int32_t> pof(fxy_of.begin(), fxy_of.end());
+        if ((s = h2d(ctx, C.G.own, pof))) return s;
+        F2M_CUDA(launch_grid_order(C.B, C.G, 0, H.V, C.G.own, true, ctx->stream, &ctx->launches));
         F2M_CUDA(launch_solve_grid(C.B, to_dev(prm), C.G, 0, H.V, false, ctx->stream, &ctx->launches));
     } else {
         // the host-assembled graph may have fewer nodes than points: re-plan

@@ -174,6 +174,26 @@ def test_grid_solver_repair_matches_oracle(ctx, oracle):
         assert r.stats["repair_steps"] == o.stats["repair_steps"] > 0
 
 
+def test_grid_solver_file_and_graph_paths(ctx, tmp_path):
+    """The grid-wide solver orders its nodes by their points: on the file path
+    (nodes in the reference's order, mapped to file points) and on the graph
+    path (no coordinates, the caller's order) it must give the per-team
+    solver's potentials bit for bit."""
+    x, y = synth.uniform_int_points(4000, 43)
+    path = str(tmp_path / "g4000.tsp")
+    synth.write_tsplib(path, x, y)
+    team = ctx.solve_file(path, 14)
+    grid = ctx.solve_file(path, 14, params=f2m_b200.default_params(solver=2))
+    assert team.status == grid.status == 0
+    assert np.array_equal(team.F, grid.F)
+    assert _close(team.lp, grid.lp) and team.max_rank == grid.max_rank
+    g = ctx.knn(x, y, 14)
+    gt = ctx.solve_graph(len(g.F), g.v1, g.v2, g.D, g.Do)
+    gg = ctx.solve_graph(len(g.F), g.v1, g.v2, g.D, g.Do, params=f2m_b200.default_params(solver=2))
+    assert gt.status == gg.status == 0
+    assert np.array_equal(gt.F, gg.F)
+
+
 def test_large_instance_uses_grid_solver(ctx, oracle):
     """20,000 clustered points (the large-instance shape at 1/5 size)."""
     x, y = synth.config2(2, n=20000)
