@@ -183,6 +183,38 @@ static __device__ int qpart_b(const Inst& I, int64_t r0, int v, HP H, int size, 
     }
     return j + 1;
 }
+// The threshold loop of qpart_ptr_EF, `while (avg < g && bump < limit) {
+// avg += 1; ++bump; }`, with the stretches where every `+= 1` is exact taken
+// in one addition: above 1 inside a binade (ulp <= 1 and no carry into the
+// next binade), and at or below -1 up to 0 (the sums are multiples of the
+// ulp below the starting magnitude).  Binade crossings and the steps across
+// zero, where `+= 1` may round, run one at a time, so avg and bump end as in
+// the plain loop.  The plain loop costs g - avg dependent FP64 additions,
+// thousands where reduced costs are large in units of the shortest edge.
+__device__ __forceinline__ void bump_until(double& avg, int& bump, double g, int limit) {
+    while (avg < g && bump < limit) {
+        long long n = 0;  // steps that stay exact
+        if (avg >= 1.0 && avg < 4503599627370496.0) {  // [1, 2^52)
+            int e;
+            frexp(avg, &e);
+            n = (long long)ceil(ldexp(1.0, e) - avg) - 1;  // avg + n < 2^e (the difference is exact)
+        } else if (avg <= -1.0 && avg > -4503599627370496.0) {
+            n = (long long)floor(-avg);  // avg + n <= 0
+        }
+        if (n >= 1) {
+            long long c = (long long)fmin(ceil(g - avg), (double)n);
+            if (c < 1) c = 1;
+            while (c > 1 && avg + (double)(c - 1) >= g) --c;  // stop where the plain loop stops
+            if (c > (long long)(limit - bump)) c = limit - bump;
+            avg += (double)c;
+            bump += (int)c;
+        } else {
+            avg += 1;
+            ++bump;
+        }
+    }
+}
+
 // qpart_ptr_EF (graph_cuda_partition.hpp:27-54): raise the threshold by 1
 // until at least ef_min entries qualify (bounded: see qpart_b).
 //
@@ -213,10 +245,7 @@ static __device__ int qpart_ef(const Inst& I, int64_t r0, int v, HP H, int size,
         avg += 1;
         ++bump;
         if (nan) continue;
-        while (avg < g && bump < kLimit) {
-            avg += 1;
-            ++bump;
-        }
+        bump_until(avg, bump, g, kLimit);
     }
     return size;
 }

@@ -173,13 +173,48 @@ __device__ __forceinline__ int qpart_ef_g(const Inst& I, int64_t r0, int v, L2Pt
         avg += 1;
         ++bump;
         if (nan) continue;
-        while (avg < g && bump < kLimit) {
-            avg += 1;
-            ++bump;
-        }
+        bump_until(avg, bump, g, kLimit);
     }
     return size;
 }
+
+// qpart_ptr_EF on a node's list copied to shared memory: `pl` holds the list
+// order and `val` the reduced cost of each position.  The loop is qpart_ef's
+// (the Hoare scans, the swaps, which move both arrays, and the threshold
+// sequence), so the final order and count are the same; only the values are
+// read from shared memory instead of three dependent global loads each.
+__device__ int qpart_b_vals(uint16_t* pl, double* val, int size, double avg) {
+    int low = 0, high = size - 1, i = low, j = high;
+    for (int pass = 0; i < j && pass <= size; ++pass) {
+        while (i <= high && val[i] <= avg) i++;
+        while (j >= low && val[j] > avg) j--;
+        if (i < j) {
+            const uint16_t t = pl[i]; pl[i] = pl[j]; pl[j] = t;
+            const double u = val[i]; val[i] = val[j]; val[j] = u;
+        }
+    }
+    return j + 1;
+}
+__device__ int qpart_ef_vals(uint16_t* pl, double* val, int size, double avg, int ef_min) {
+    if (size < ef_min) return size;
+    constexpr int kLimit = 1 << 20;
+    for (int bump = 0; bump < kLimit;) {
+        const int p = qpart_b_vals(pl, val, size, avg);
+        if (p >= ef_min) return p;
+        double g = INFINITY;
+        bool nan = false;
+        for (int k = 0; k < size; ++k) {
+            nan |= (val[k] != val[k]);
+            if (k >= p) g = fmin(g, val[k]);
+        }
+        avg += 1;
+        ++bump;
+        if (nan) continue;
+        bump_until(avg, bump, g, kLimit);
+    }
+    return size;
+}
+constexpr int kPartCap = 128;  // longest list partitioned in shared memory by a warp
 
 // Open-addressing table node -> local index in shared memory (the halo
 // build).  An entry is (node << 32 | local index); node ids are below 2^31,
@@ -581,12 +616,65 @@ struct GridSolver {
         }
     }
 
-    __device__ double check_opt() {
-        for (int i = threadIdx.x; i < nown(); i += kGT) {
+    // update_EF's partitions of the own nodes' lists (cuda_partition_v2 with
+    // threshold thr, or v4 with the largest of the first glob_K reduced costs
+    // when glob): warp w takes the own nodes w, w+32, ...; a list of up to
+    // kPartCap entries is copied with its reduced costs into the warp's
+    // shared scratch in one parallel round of loads and partitioned there by
+    // one lane (the halo region is free here: it is rebuilt after every
+    // update_EF).  Without the scratch, or for longer lists, one lane runs
+    // the global-memory partition.
+    __device__ void partition_own(bool glob, double thr) {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const bool scratch = L.nl > 0 && (long long)L.ne * 12 >= 32LL * kPartCap * 10;
+        double* val = L.D + wid * kPartCap;
+        uint16_t* pl = reinterpret_cast<uint16_t*>(L.D + 32 * kPartCap) + wid * kPartCap;
+        const L2Ptr H = hc();
+        for (int i = wid; i < nown(); i += kGT / 32) {
             const int v = node(i);
             const int d = deg(v);
-            G.efc[v] = (d < P.ef_small_deg) ? d : qpart_ef_g(I, I.row[v], v, hc(), d, P.ef_thr, P.ef_min);
+            if (glob ? d < P.glob_K : d < P.ef_small_deg) {
+                if (lane == 0) G.efc[v] = d;
+                continue;
+            }
+            const int64_t r0 = I.row[v];
+            uint16_t* list = I.perm + r0;
+            int p = 0;
+            if (scratch && d <= kPartCap) {
+                const double hv = H[v];
+                for (int k = lane; k < d; k += 32) {
+                    const uint16_t q = list[k];
+                    pl[k] = q;
+                    val[k] = red_d(I.slot[r0 + q], v, H, hv);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    double avg = thr;
+                    if (glob) {
+                        avg = val[0];
+                        for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, val[k]);
+                    }
+                    p = qpart_ef_vals(pl, val, d, avg, P.ef_min);
+                }
+                __syncwarp();
+                for (int k = lane; k < d; k += 32) list[k] = pl[k];
+                __syncwarp();
+            } else if (lane == 0) {
+                double avg = thr;
+                if (glob) {
+                    const double hv = H[v];
+                    avg = pdv(I, r0, list, 0, v, H, hv);
+                    for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, list, k, v, H, hv));
+                }
+                p = qpart_ef_g(I, r0, v, H, d, avg, P.ef_min);
+            }
+            if (lane == 0) G.efc[v] = p;
         }
+        __syncthreads();
+    }
+
+    __device__ double check_opt() {
+        partition_own(false, P.ef_thr);
         rebuild_ef();
         checks++;
         return grad_max();
@@ -605,16 +693,7 @@ struct GridSolver {
         rebuild_ef();
         for (int go = 0; go < P.glob_rounds && !dead; ++go) {
             steps(P.glob_inner);
-            for (int i = threadIdx.x; i < nown(); i += kGT) {
-                const int v = node(i);
-                const int d = deg(v);
-                if (d < P.glob_K) { G.efc[v] = d; continue; }
-                const int64_t r0 = I.row[v];
-                const double hv = hc()[v];
-                double avg = pdv(I, r0, I.perm + r0, 0, v, hc(), hv);
-                for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, I.perm + r0, k, v, hc(), hv));
-                G.efc[v] = qpart_ef_g(I, r0, v, hc(), d, avg, P.ef_min);
-            }
+            partition_own(true, 0.0);
             rebuild_ef();
             if (grad_max() < P.glob_tol) break;
         }
