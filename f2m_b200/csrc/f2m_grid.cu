@@ -1054,4 +1054,57 @@ cudaError_t launch_grid_order(const Batch& B, const GridState& G, int b, int V, 
     return cudaGetLastError();
 }
 
+/* ------------------------------------------------------------------ */
+/* the reference's edge order of one instance                           */
+/* ------------------------------------------------------------------ */
+// Per slot of node v: keys (emitter << 32 | partner) and the cost's bits
+// (costs are non-negative, so their bits order as the values) for a slot
+// whose neighbour is the higher id, all ones (last) otherwise.
+__global__ void k_edge_keys(Batch B, int b, int V, unsigned long long* k1, uint32_t* v1) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int64_t base = B.offs[b];
+    const int64_t s0 = B.row[base];
+    for (int64_t a = B.row[base + v]; a < B.row[base + v + 1]; ++a) {
+        const bool up = B.slot[a].nbr > v;
+        k1[a - s0] = up ? (((unsigned long long)(unsigned)B.s_em[a] << 32) | (unsigned)B.s_oth[a]) : ~0ull;
+        v1[a - s0] = (uint32_t)(a - s0);
+    }
+}
+__global__ void k_edge_cost_keys(Batch B, int b, int64_t S, const unsigned long long* k1, const uint32_t* v1,
+                                 unsigned long long* k2) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S) return;
+    const int64_t s0 = B.row[B.offs[b]];
+    k2[i] = k1[i] == ~0ull ? ~0ull : (unsigned long long)__double_as_longlong(B.s_cost[s0 + v1[i]]);
+}
+
+size_t edge_order_temp_bytes(int64_t S) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                    (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)S);
+    return bytes;
+}
+
+cudaError_t launch_edge_order(const Batch& B, int b, int V, int64_t S, const EdgeSort& E, const uint32_t** order,
+                              cudaStream_t s, int64_t* launches) {
+    if (V <= 0 || S <= 0) { *order = E.v2; return cudaSuccess; }
+    const int T = 256;
+    k_edge_keys<<<(V + T - 1) / T, T, 0, s>>>(B, b, V, E.k1, E.v1);
+    ++*launches;
+    // LSD: by (emitter, partner), then stably by cost
+    size_t bytes = E.tmp_bytes;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(E.tmp, bytes, E.k1, E.k2, E.v1, E.v2, (int)S, 0, 64, s);
+    if (e != cudaSuccess) return e;
+    ++*launches;
+    k_edge_cost_keys<<<(unsigned)((S + T - 1) / T), T, 0, s>>>(B, b, S, E.k2, E.v2, E.k1);
+    ++*launches;
+    bytes = E.tmp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(E.tmp, bytes, E.k1, E.k2, E.v2, E.v1, (int)S, 0, 64, s);
+    if (e != cudaSuccess) return e;
+    ++*launches;
+    *order = E.v1;
+    return cudaGetLastError();
+}
+
 }  // namespace f2m

@@ -152,6 +152,23 @@ cudaError_t launch_solve_grid(const Batch& B, const DevParams& P, const GridStat
 cudaError_t launch_grid_order(const Batch& B, const GridState& G, int b, int V, const int32_t* point_of,
                               bool spatial, cudaStream_t s, int64_t* launches);
 size_t grid_order_temp_bytes(int64_t n);
+
+// Buffers of the device edge order of one instance (single-instance calls).
+struct EdgeSort {
+    unsigned long long* k1;  // [S] keys
+    unsigned long long* k2;  // [S]
+    uint32_t* v1;            // [S] slot offsets within the instance
+    uint32_t* v2;            // [S]
+    void* tmp;               // radix-sort scratch
+    size_t tmp_bytes;
+};
+size_t edge_order_temp_bytes(int64_t S);
+// The reference's edge order (ascending cost, then emitter, then partner:
+// graph_tour.hpp:28-98) of instance b's edges, each as the offset of its slot
+// in the lower-id endpoint's list (within the instance's slots); the first
+// S/2 entries of *order are the edges in order.
+cudaError_t launch_edge_order(const Batch& B, int b, int V, int64_t S, const EdgeSort& E, const uint32_t** order,
+                              cudaStream_t s, int64_t* launches);
 cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches);
 cudaError_t launch_knn(const Batch& B, int64_t* scan_scratch, cudaStream_t s, int64_t* launches);
 cudaError_t launch_graph(const Batch& B, int64_t* deg_scratch, int64_t* scan_scratch,

@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iomanip>
@@ -371,6 +372,71 @@ void parallel_sort(std::vector<T>& a, Less less) {
     }
 }
 
+// get_KXY's rounding and de-duplication (FXY.hpp:252-267): coordinates
+// rounded to 1e-3 and the first occurrence of each rounded point kept, in
+// input order.  A sort of the rounded points (ties by input index) finds the
+// repeats instead of the reference's nested hash maps; +0 and -0 compare
+// equal and a point with a NaN coordinate is never a repeat, as there.
+void host_dedup_points(const double* x, const double* y, const int32_t* labels, int32_t n,
+                       std::vector<double>& hx, std::vector<double>& hy, std::vector<int32_t>& hl) {
+    std::vector<double> rx(n), ry(n);
+    parallel_for(n, [&](int64_t i0, int64_t i1) {
+        for (int64_t i = i0; i < i1; ++i) {
+            double xx = std::round(x[i] * 1000), yy = std::round(y[i] * 1000);
+            rx[i] = xx / 1000;
+            ry[i] = yy / 1000;
+        }
+    });
+    auto nanp = [&](int32_t i) { return rx[i] != rx[i] || ry[i] != ry[i]; };
+    std::vector<int32_t> idx(n);
+    for (int32_t i = 0; i < n; ++i) idx[i] = i;
+    parallel_sort(idx, [&](int32_t a, int32_t b) {
+        const bool na = nanp(a), nb = nanp(b);
+        if (na != nb) return nb;
+        if (!na) {
+            if (rx[a] != rx[b]) return rx[a] < rx[b];
+            if (ry[a] != ry[b]) return ry[a] < ry[b];
+        }
+        return a < b;
+    });
+    std::vector<char> dup(n, 0);
+    for (int32_t k = 1; k < n; ++k) {
+        const int32_t a = idx[k - 1], b = idx[k];
+        if (!nanp(a) && !nanp(b) && rx[a] == rx[b] && ry[a] == ry[b]) dup[b] = 1;
+    }
+    hx.clear();
+    hy.clear();
+    hl.clear();
+    for (int32_t i = 0; i < n; ++i) {
+        if (dup[i]) continue;
+        hx.push_back(rx[i]);
+        hy.push_back(ry[i]);
+        hl.push_back(labels ? labels[i] : i + 1);
+    }
+}
+
+// Host stage times of one call, printed to stderr when F2M_HOST_TIMING is
+// set (the device phases have their own CUDA-event timers).
+struct StageClock {
+    bool on = std::getenv("F2M_HOST_TIMING") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    std::string line;
+    void mark(const char* name) {
+        if (!on) return;
+        const auto now = std::chrono::steady_clock::now();
+        char buf[64];
+        std::snprintf(buf, sizeof(buf), " %s=%.2f", name, std::chrono::duration<double, std::milli>(now - t).count());
+        line += buf;
+        t = now;
+    }
+    ~StageClock() {
+        if (on && !line.empty()) std::fprintf(stderr, "f2m host stages (ms):%s\n", line.c_str());
+    }
+};
+
+template <class SlotOf>
+void fill_edges(HostInst& H, int64_t E, SlotOf slot_of);
+
 void number_edges(HostInst& H, const std::vector<int>& em, const std::vector<int>& oth) {
     Range rg("f2m number edges");
     struct K { double c; int e, o; int v; int64_t s; };
@@ -397,15 +463,30 @@ void number_edges(HostInst& H, const std::vector<int>& em, const std::vector<int
         if (x.e != y.e) return x.e < y.e;
         return x.o < y.o;
     });
-    H.E = (int)ks.size();
+    fill_edges(H, (int64_t)ks.size(), [&](int64_t e) { return ks[e].s; });
+}
+
+// The same numbering from the edge order computed on the device
+// (launch_edge_order): ord[e] is the slot of edge e in its lower-id
+// endpoint's list.
+void number_edges_ordered(HostInst& H, const uint32_t* ord, int64_t E) {
+    Range rg("f2m number edges");
+    fill_edges(H, E, [&](int64_t e) { return (int64_t)ord[e]; });
+}
+
+// Edge arrays of H from the edges in order, each given by its slot in the
+// lower-id endpoint's list (the endpoint is found through the mirror slot).
+template <class SlotOf>
+void fill_edges(HostInst& H, int64_t E, SlotOf slot_of) {
+    H.E = (int)E;
     H.slot_edge.assign(H.nbr.size(), -1);
     H.ev1.resize(H.E); H.ev2.resize(H.E); H.el1.resize(H.E); H.el2.resize(H.E);
     H.rank1.resize(H.E); H.rank2.resize(H.E); H.eD.resize(H.E); H.eDo.resize(H.E);
     parallel_for(H.E, [&](int64_t e0, int64_t e1) {
     for (int64_t e = e0; e < e1; ++e) {
-        const int v = ks[e].v;
-        const int64_t a = ks[e].s;
+        const int64_t a = slot_of(e);
         const int u = H.nbr[a];
+        const int v = H.nbr[H.row[u] + H.mirror[a]];
         H.slot_edge[a] = e;
         H.slot_edge[H.row[u] + H.mirror[a]] = e;
         H.ev1[e] = v; H.ev2[e] = u;
@@ -664,7 +745,18 @@ struct DevCall {
     int64_t* deg = nullptr;
     int64_t* scan = nullptr;
     int32_t *ci = nullptr, *cs = nullptr, *ord = nullptr;
+    EdgeSort es{};          // device edge order buffers (single-instance calls)
+    bool has_es = false;
 };
+
+void carve_edge_sort(Arena& A, EdgeSort& E, int64_t S) {
+    E.k1 = A.take<unsigned long long>(S);
+    E.k2 = A.take<unsigned long long>(S);
+    E.v1 = A.take<uint32_t>(S);
+    E.v2 = A.take<uint32_t>(S);
+    E.tmp_bytes = edge_order_temp_bytes(S);
+    E.tmp = A.take<unsigned char>(E.tmp_bytes);
+}
 
 f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h_offs, int32_t top_k,
                       const f2m_params& prm, bool own_inputs) {
@@ -675,13 +767,16 @@ f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h
                                                std::to_string(solve_max_nodes()) +
                                                " points each; solve larger ones one at a time");
     Arena A;
+    C.has_es = n_inst == 1;
     carve(A, C.B, C.pl, own_inputs, &C.deg, &C.scan, &C.ci, &C.cs, &C.ord);
     if (C.grid) carve_grid(A, C.G, std::max<int64_t>(C.pl.n_total, 1), C.B.S_cap);
+    if (C.has_es) carve_edge_sort(A, C.es, std::max<int64_t>(C.B.S_cap, 1));
     F2M_CUDA(ensure_device(ctx, A.used));
     A.base = ctx->dev;
     A.used = 0;
     carve(A, C.B, C.pl, own_inputs, &C.deg, &C.scan, &C.ci, &C.cs, &C.ord);
     if (C.grid) carve_grid(A, C.G, std::max<int64_t>(C.pl.n_total, 1), C.B.S_cap);
+    if (C.has_es) carve_edge_sort(A, C.es, std::max<int64_t>(C.B.S_cap, 1));
     C.B.skip_dedup = 0;
     C.B.cost_mode = prm.cost_mode;
     // work lists through pinned staging
@@ -795,7 +890,12 @@ f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, boo
     F2M_CUDA(cp(cost, B.s_cost + s0, S * 8));
     F2M_CUDA(cp(mirror, B.mirror + s0, S * 4));
     F2M_CUDA(cp(perm, B.perm + s0, S * 2));
-    if (with_keys) {
+    const bool dev_order = with_keys && C.has_es;
+    if (dev_order) {  // the edge order sorted on the device: one array back
+        const uint32_t* ord = nullptr;
+        F2M_CUDA(launch_edge_order(B, b, V, S, C.es, &ord, ctx->stream, &ctx->launches));
+        F2M_CUDA(cp(em, ord, (S / 2) * 4));
+    } else if (with_keys) {
         F2M_CUDA(cp(em, B.s_em + s0, S * 4));
         F2M_CUDA(cp(oth, B.s_oth + s0, S * 4));
     }
@@ -804,6 +904,7 @@ f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, boo
     F2M_CUDA(cp(ccnt, B.ccnt + base, V * 4));
     F2M_CUDA(cp(K, B.K + base, V * 4));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    StageClock clk;
     H.row.resize(V + 1);
     for (int v = 0; v <= V; ++v) H.row[v] = row[v] - s0;
     H.nbr.resize(S);
@@ -818,11 +919,18 @@ f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, boo
     H.efcnt.assign(efcnt, efcnt + V);
     H.ccnt.assign(ccnt, ccnt + V);
     H.label.assign(K, K + V);
-    if (with_keys) {
+    clk.mark("pull.unpack");
+    if (dev_order) {
+        std::vector<uint32_t> ord(reinterpret_cast<uint32_t*>(em), reinterpret_cast<uint32_t*>(em) + S / 2);
+        if (lk.owns_lock()) lk.unlock();  // the staging is no longer needed
+        number_edges_ordered(H, ord.data(), S / 2);
+        clk.mark("pull.number_edges");
+    } else if (with_keys) {
         std::vector<int> ev(em, em + S), ov(oth, oth + S);
         if (lk.owns_lock()) lk.unlock();  // the staging is no longer needed
         // keys hold FXY indices; node ids here are the same indices
         number_edges(H, ev, ov);
+        clk.mark("pull.number_edges");
     }
     return F2M_OK;
 }
@@ -832,8 +940,11 @@ f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& 
     Range rg("f2m complete instance");
     HostInst& H = R.H;
     const double vb = prm.error_B * prm.error_B_comb;
+    StageClock clk;
     HostCheck HC(H, vb);
+    clk.mark("hostcheck.build");
     int IRR_B = HC.check();
+    clk.mark("hostcheck.check");
     int steps = 0;
     if (IRR_B > 0) {
         // the repair steps use the call's stream and work lists: one host
@@ -893,6 +1004,7 @@ f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& 
     R.st.irr_a = HC.irr_a;
     R.st.irr_b = IRR_B > 0 ? IRR_B : 0;
     R.st.n_combs = (int32_t)HC.comb_V.size();
+    clk.mark("repair");
     R.x.assign(H.E, 0.0);
     R.X.clear();
     if (IRR_B == 0) {
@@ -931,6 +1043,7 @@ f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& 
         R.err = "Optimal Solution not Found";
         R.lp = NAN;
     }
+    clk.mark("primal");
     // FP64 dual bound with u = -F/2 in d_min units
     double fsum = 0, neg = 0;
     for (int v = 0; v < H.V; ++v) fsum += H.F[v];
@@ -940,6 +1053,7 @@ f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& 
     }
     R.st.dual_value = H.dmin * (-fsum + neg);
     R.st.d_min = H.dmin;
+    clk.mark("dual");
     return F2M_OK;
 }
 
@@ -1318,24 +1432,15 @@ f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int
     std::vector<double> hx, hy;
     std::vector<int32_t> hl;
     bool host_dedup = n > kHostDedupPoints;
+    StageClock clk;
     if (host_dedup) {
-        std::unordered_map<double, std::unordered_map<double, int>> filtr;
-        for (int32_t i = 0; i < n; ++i) {
-            double xx = std::round(x[i] * 1000), yy = std::round(y[i] * 1000);
-            xx /= 1000;
-            yy /= 1000;
-            auto fx = filtr.find(xx);
-            if (fx != filtr.end() && fx->second.count(yy)) continue;
-            filtr[xx][yy] = i;
-            hx.push_back(xx);
-            hy.push_back(yy);
-            hl.push_back(labels ? labels[i] : i + 1);
-        }
+        host_dedup_points(x, y, labels, n, hx, hy, hl);
         x = hx.data();
         y = hy.data();
         labels = hl.data();
         n = (int32_t)hx.size();
     }
+    clk.mark("dedup");
     const int64_t offs2[2] = {0, n};
     DevCall C;
     if ((s = setup_call(ctx, C, 1, offs2, top_k, prm, true))) return s;
@@ -1382,6 +1487,7 @@ f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int
         *out = R.release();
         return F2M_OK;
     }
+    clk.mark("setup");
     if ((s = launch_classes(ctx, C, prm))) return s;
     F2M_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
     ctx->timed = true;
@@ -1389,6 +1495,7 @@ f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int
     int32_t st = 0;
     F2M_CUDA(cudaMemcpyAsync(&st, C.B.status, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    clk.mark("device");
     if (st != F2M_OK && st != kNeedsHost) {
         R->status = st;
         R->err = st == F2M_ERR_INPUT ? "invalid instance (fewer than 4 distinct points or degenerate box)"
@@ -1397,8 +1504,10 @@ f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int
         return (f2m_status)st;
     }
     if ((s = pull_instance(ctx, C, 0, R->H, true))) return s;
+    clk.mark("pull");
     if ((s = pull_stats(ctx, C, 0, *R))) return s;
     if ((s = complete_instance(ctx, C, 0, prm, *R))) return s;
+    clk.mark("complete");
     if ((s = pull_stats(ctx, C, 0, *R))) return s;
     R->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = R.release();
