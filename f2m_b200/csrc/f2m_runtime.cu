@@ -1057,6 +1057,75 @@ f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& 
     return F2M_OK;
 }
 
+// The primal of an instance whose combs the device found all regular
+// (2A+B = 4 at every comb node, status F2M_OK): then every comb's solution is
+// x = 1/2 on its half edges (comb_thread.cpp solve_simple), which is the
+// device's per-slot code (xcode), so the host comb stage would change
+// nothing.  x, MAX rank, the degree check and the dual bound are taken as
+// complete_instance takes them, and OVAL is summed in edge-id order (the
+// host stage sums in graph::X's hash order; the two agree to rounding);
+// comb counts come from the device.  Used by the points path; the file
+// path keeps the host stage, which also writes the reference's files.
+f2m_status complete_from_device(f2m_ctx* ctx, const DevCall& C, int b, f2m_result& R) {
+    Range rg("f2m complete instance (device combs)");
+    HostInst& H = R.H;
+    int64_t base = 0, s0 = 0;
+    int32_t nc = 0;
+    F2M_CUDA(cudaMemcpyAsync(&base, C.B.offs + b, sizeof(base), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(&s0, C.B.row + base, sizeof(s0), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(&nc, C.B.n_combs + b, sizeof(nc), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    const int64_t S = (int64_t)H.nbr.size();
+    F2M_CUDA(ensure_pinned(ctx, (size_t)std::max<int64_t>(S, 1)));
+    F2M_CUDA(cudaMemcpyAsync(ctx->pinned, C.B.xcode + s0, S, cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    const uint8_t* xc = reinterpret_cast<const uint8_t*>(ctx->pinned);
+    R.x.assign(H.E, 0.0);
+    parallel_for(H.E, [&](int64_t e0, int64_t e1) {
+        for (int64_t e = e0; e < e1; ++e) {
+            const int v = H.ev1[e];
+            const int64_t a = H.row[v] + (H.el1[e] == v ? H.rank1[e] : H.rank2[e]);
+            const uint8_t c = xc[a];
+            R.x[e] = c == 2 ? 1.0 : (c == 1 ? 0.5 : 0.0);
+        }
+    });
+    R.X.clear();
+    double OVAL = 0;  // graph::getOVAL (graph_tour.hpp:165-184)
+    int mr = 0;
+    std::vector<float> deg(H.V, 0.0f);
+    std::vector<char> has(H.V, 0);
+    for (int e = 0; e < H.E; ++e) {
+        const double x = R.x[e];
+        if (x == 0.0) continue;
+        R.X.emplace(e, x);
+        mr = std::max(mr, std::min(H.rank1[e], H.rank2[e]));
+        OVAL += x * H.eDo[e];
+        deg[H.el1[e]] += (float)x; has[H.el1[e]] = 1;
+        deg[H.el2[e]] += (float)x; has[H.el2[e]] = 1;
+    }
+    int viol = 0;  // graph::check_solution (graph_tour.hpp:142-163)
+    for (int v = 0; v < H.V; ++v)
+        if (has[v] && !(deg[v] > 2.0f - 1e-2f && deg[v] < 2.0f + 1e-2f)) viol++;
+    R.lp = OVAL;
+    R.max_rank = mr;
+    R.status = F2M_OK;
+    R.st.repair_steps = 0;
+    R.st.irr_a = 0;
+    R.st.irr_b = 0;
+    R.st.n_combs = nc;
+    R.st.degree_violations = viol;
+    double fsum = 0, neg = 0;  // FP64 dual bound, as complete_instance
+    for (int v = 0; v < H.V; ++v) fsum += H.F[v];
+    for (int e = 0; e < H.E; ++e) {
+        const double d = (H.eD[e] + 0.5 * H.F[H.ev1[e]]) + 0.5 * H.F[H.ev2[e]];
+        neg += std::min(0.0, d);
+    }
+    R.st.dual_value = H.dmin * (-fsum + neg);
+    R.st.d_min = H.dmin;
+    return F2M_OK;
+}
+
 f2m_status pull_stats(f2m_ctx* ctx, const DevCall& C, int b, f2m_result& R) {
     int64_t it = 0;
     int32_t ch = 0;
@@ -1506,7 +1575,10 @@ f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int
     if ((s = pull_instance(ctx, C, 0, R->H, true))) return s;
     clk.mark("pull");
     if ((s = pull_stats(ctx, C, 0, *R))) return s;
-    if ((s = complete_instance(ctx, C, 0, prm, *R))) return s;
+    // regular combs only: the device's primal stands; otherwise the host comb
+    // stage (Ax=b, repair loop) as the reference runs it
+    if ((s = (st == F2M_OK ? complete_from_device(ctx, C, 0, *R) : complete_instance(ctx, C, 0, prm, *R))))
+        return s;
     clk.mark("complete");
     if ((s = pull_stats(ctx, C, 0, *R))) return s;
     R->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
