@@ -371,3 +371,28 @@ def test_resume_from_stored_potentials(ctx):
         with pytest.raises(f2m_b200.F2MError) as e:
             ctx.solve_points_from(x, y, N, r1.F[:-1])
         assert e.value.status == f2m_b200.ERR_INPUT
+
+
+def test_grid_block_depths_give_identical_potentials(tmp_path):
+    """Halo blocks recompute the nodes within k EF hops of each CTA's own
+    nodes so that one grid barrier covers k Jacobi steps: the potentials must
+    not depend on k (0 = one grid barrier per step).  The depth is read once
+    per process, so each depth runs in a child process."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import f2m_b200; from f2m_b200 import synth; "
+            "x, y = synth.config2(5, n=20000); r = f2m_b200.Context(0).solve_points(x, y, 16, "
+            "params=f2m_b200.default_params(solver=2)); np.savez(sys.argv[1], F=r.F, x=r.x, lp=r.lp, "
+            "it=r.stats['iterations'])" % root)
+    out = {}
+    for k in (0, 2, 8):
+        f = str(tmp_path / f"k{k}.npz")
+        env = dict(os.environ, F2M_GRID_BLOCK=str(k))
+        subprocess.run([sys.executable, "-c", code, f], env=env, check=True, timeout=600)
+        out[k] = np.load(f)
+    for k in (2, 8):
+        assert np.array_equal(out[k]["F"], out[0]["F"]), f"depth {k} changed the potentials"
+        assert np.array_equal(out[k]["x"], out[0]["x"])
+        assert int(out[k]["it"]) == int(out[0]["it"])
+        assert _close(float(out[k]["lp"]), float(out[0]["lp"]))
