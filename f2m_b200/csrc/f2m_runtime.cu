@@ -333,9 +333,9 @@ struct HostInst {
 // fn(begin, end) over [0, n) in contiguous ranges on up to 32 host threads
 // (inline below 20,000 items)
 template <class Fn>
-void parallel_for(int64_t n, Fn fn) {
+void parallel_for(int64_t n, Fn fn, int64_t serial_below = 20000) {
     const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const int64_t T = (n < 20000) ? 1 : std::min<int64_t>(std::min<int64_t>(hw, 32), n);
+    const int64_t T = (n < serial_below) ? 1 : std::min<int64_t>(std::min<int64_t>(hw, 32), n);
     if (T <= 1) { fn((int64_t)0, n); return; }
     std::vector<std::thread> pool;
     for (int64_t t = 1; t < T; ++t) pool.emplace_back(fn, n * t / T, n * (t + 1) / T);
@@ -646,20 +646,28 @@ struct HostCheck {
         extract_combs();
         Combs.clear();
         Combs.resize(comb_V.size());
-        std::vector<int> irrA;
-        for (size_t c = 0; c < comb_V.size(); ++c) {  // COMB_thread + solve_simple
-            auto& C = Combs[c];
-            for (int v : comb_V[c]) C.nodes[v]++;
-            for (auto& kv : C.nodes)
-                if (4 - 2 * sA[kv.first] - sB[kv.first] != 0) { C.STATUS = -1; break; }
-            if (C.STATUS == 1)
+        // combs are independent: each is built and solved by one thread, in
+        // the reference's order inside the comb (its maps' insertion order,
+        // which the Ax=b rows follow)
+        parallel_for((int64_t)comb_V.size(), [&](int64_t c0, int64_t c1) {
+            for (int64_t c = c0; c < c1; ++c) {  // COMB_thread + solve_simple
+                auto& C = Combs[c];
+                for (int v : comb_V[c]) C.nodes[v]++;
                 for (auto& kv : C.nodes)
-                    for (int e : eB[kv.first]) C.XB[e] = 0.5f;
-            else irrA.push_back((int)c);
-        }
+                    if (4 - 2 * sA[kv.first] - sB[kv.first] != 0) { C.STATUS = -1; break; }
+                if (C.STATUS == 1)
+                    for (auto& kv : C.nodes)
+                        for (int e : eB[kv.first]) C.XB[e] = 0.5f;
+            }
+        }, 256);
+        std::vector<int> irrA;
+        for (size_t c = 0; c < comb_V.size(); ++c)
+            if (Combs[c].STATUS != 1) irrA.push_back((int)c);
         irr_a = (int)irrA.size();
         if (!irrA.empty()) {
-            for (int c : irrA) {  // comb::solve_AxB (comb_thread.cpp:272-304)
+            parallel_for((int64_t)irrA.size(), [&](int64_t j0, int64_t j1) {
+            for (int64_t jj = j0; jj < j1; ++jj) {  // comb::solve_AxB (comb_thread.cpp:272-304)
+                const int c = irrA[jj];
                 auto& C = Combs[c];
                 std::vector<int> rows;
                 std::unordered_map<int, int> mapX, mapXR;
@@ -681,6 +689,7 @@ struct HostCheck {
                 C.AxB_status = ab.go_max;
                 for (size_t j = 0; j < ab.x.size(); j++) C.XB[mapXR[(int)j]] = (float)ab.x[j];
             }
+            }, 2);
             irrB.clear();  // get_comb_IRREGULAR_B
             for (size_t c = 0; c < Combs.size(); ++c)
                 if (Combs[c].AxB_status == 0) irrB.push_back((int)c);
