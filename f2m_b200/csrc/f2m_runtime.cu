@@ -346,18 +346,21 @@ void parallel_for(int64_t n, Fn fn, int64_t serial_below = 20000) {
 // std::sort of a large array as sorted chunks merged pairwise, each level's
 // merges side by side (the keys here are unique, so the order is the same)
 template <class T, class Less>
-void parallel_sort(std::vector<T>& a, Less less) {
+void parallel_sort(std::vector<T>& a, Less less, int64_t serial_below = 200000) {
     const int64_t n = (int64_t)a.size();
     const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
     int64_t parts = 1;
     while (parts * 2 <= std::min<int64_t>(hw, 32)) parts *= 2;
-    if (n < 200000 || parts < 2) { std::sort(a.begin(), a.end(), less); return; }
+    if (n < serial_below || parts < 2) { std::sort(a.begin(), a.end(), less); return; }
     std::vector<int64_t> b(parts + 1);
     for (int64_t p = 0; p <= parts; ++p) b[p] = n * p / parts;
-    parallel_for(parts * 20000, [&](int64_t i0, int64_t i1) {
-        for (int64_t p = i0 / 20000; p < (i1 + 19999) / 20000 && p < parts; ++p)
-            if (p * 20000 >= i0) std::sort(a.begin() + b[p], a.begin() + b[p + 1], less);
-    });
+    {
+        std::vector<std::thread> pool;
+        for (int64_t p = 1; p < parts; ++p)
+            pool.emplace_back([&, p] { std::sort(a.begin() + b[p], a.begin() + b[p + 1], less); });
+        std::sort(a.begin() + b[0], a.begin() + b[1], less);
+        for (auto& th : pool) th.join();
+    }
     std::vector<T> tmp(n);
     for (int64_t w = 1; w < parts; w *= 2) {
         const int64_t pairs = parts / (2 * w);
@@ -398,7 +401,7 @@ void host_dedup_points(const double* x, const double* y, const int32_t* labels, 
             if (ry[a] != ry[b]) return ry[a] < ry[b];
         }
         return a < b;
-    });
+    }, 50000);
     std::vector<char> dup(n, 0);
     for (int32_t k = 1; k < n; ++k) {
         const int32_t a = idx[k - 1], b = idx[k];
@@ -921,9 +924,14 @@ f2m_status pull_instance(f2m_ctx* ctx, const DevCall& C, int b, HostInst& H, boo
     parallel_for(S, [&](int64_t a0, int64_t a1) {
         for (int64_t a = a0; a < a1; ++a) { H.nbr[a] = sl[a].nbr; H.Dn[a] = sl[a].D; }
     });
-    H.cost.assign(cost, cost + S);
-    H.perm.assign(perm, perm + S);
-    H.mirror.assign(mirror, mirror + S);
+    H.cost.resize(S);
+    H.perm.resize(S);
+    H.mirror.resize(S);
+    parallel_for(S, [&](int64_t a0, int64_t a1) {
+        std::memcpy(H.cost.data() + a0, cost + a0, (a1 - a0) * sizeof(double));
+        std::memcpy(H.perm.data() + a0, perm + a0, (a1 - a0) * sizeof(uint16_t));
+        std::memcpy(H.mirror.data() + a0, mirror + a0, (a1 - a0) * sizeof(int32_t));
+    });
     H.F.assign(F, F + V);
     H.efcnt.assign(efcnt, efcnt + V);
     H.ccnt.assign(ccnt, ccnt + V);
@@ -2229,15 +2237,17 @@ double f2m_result_seconds(const f2m_result* r) { return r->seconds; }
 void f2m_result_edges(const f2m_result* r, int32_t* v1, int32_t* v2, int32_t* lab1, int32_t* lab2,
                       double* Do, double* D, double* x) {
     const HostInst& H = r->H;
-    for (int e = 0; e < H.E; ++e) {
-        if (v1) v1[e] = H.ev1[e];
-        if (v2) v2[e] = H.ev2[e];
-        if (lab1) lab1[e] = H.label[H.el1[e]];
-        if (lab2) lab2[e] = H.label[H.el2[e]];
-        if (Do) Do[e] = H.eDo[e];
-        if (D) D[e] = H.eD[e];
-        if (x) x[e] = e < (int)r->x.size() ? r->x[e] : 0.0;
-    }
+    parallel_for(H.E, [&](int64_t e0, int64_t e1) {
+        for (int64_t e = e0; e < e1; ++e) {
+            if (v1) v1[e] = H.ev1[e];
+            if (v2) v2[e] = H.ev2[e];
+            if (lab1) lab1[e] = H.label[H.el1[e]];
+            if (lab2) lab2[e] = H.label[H.el2[e]];
+            if (Do) Do[e] = H.eDo[e];
+            if (D) D[e] = H.eD[e];
+            if (x) x[e] = e < (int64_t)r->x.size() ? r->x[e] : 0.0;
+        }
+    });
 }
 void f2m_result_nodes(const f2m_result* r, int32_t* label, double* F) {
     for (int v = 0; v < r->H.V; ++v) {
