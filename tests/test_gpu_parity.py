@@ -396,3 +396,20 @@ def test_grid_block_depths_give_identical_potentials(tmp_path):
         assert np.array_equal(out[k]["x"], out[0]["x"])
         assert int(out[k]["it"]) == int(out[0]["it"])
         assert _close(float(out[k]["lp"]), float(out[0]["lp"]))
+
+
+def test_repeated_calls_are_bit_identical(ctx):
+    """Replays: every reduction here has a fixed order (team sums, the grid
+    solver's per-CTA partials read in CTA order), so the same call gives the
+    same bits, LP values included -- the check that stands in for a race
+    detector on this GPU."""
+    offs, x, y = synth.config3(seed=9, n_inst=96, hi=3000)
+    a = ctx.solve_batch(offs, x, y, 16, details=True)
+    b = ctx.solve_batch(offs, x, y, 16, details=True)
+    for k in a:
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]), equal_nan=True), k
+    gx, gy = synth.config2(6, n=20000)
+    r1 = ctx.solve_points(gx, gy, 16)
+    r2 = ctx.solve_points(gx, gy, 16)
+    assert np.array_equal(r1.F, r2.F) and np.array_equal(r1.x, r2.x)
+    assert r1.lp == r2.lp and r1.stats == r2.stats
