@@ -622,14 +622,32 @@ struct GridSolver {
     // kPartCap entries is copied with its reduced costs into the warp's
     // shared scratch in one parallel round of loads and partitioned there by
     // one lane (the halo region is free here: it is rebuilt after every
-    // update_EF).  Without the scratch, or for longer lists, one lane runs
-    // the global-memory partition.
+    // update_EF); one lane runs the global-memory partition for a longer
+    // list.  Without the scratch (no halo), a thread per node partitions in
+    // global memory.
     __device__ void partition_own(bool glob, double thr) {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
         const bool scratch = L.nl > 0 && (long long)L.ne * 12 >= 32LL * kPartCap * 10;
         double* val = L.D + wid * kPartCap;
         uint16_t* pl = reinterpret_cast<uint16_t*>(L.D + 32 * kPartCap) + wid * kPartCap;
         const L2Ptr H = hc();
+        if (!scratch) {  // no shared scratch: a thread per node, in global memory
+            for (int i = threadIdx.x; i < nown(); i += kGT) {
+                const int v = node(i);
+                const int d = deg(v);
+                if (glob ? d < P.glob_K : d < P.ef_small_deg) { G.efc[v] = d; continue; }
+                const int64_t r0 = I.row[v];
+                double avg = thr;
+                if (glob) {
+                    const double hv = H[v];
+                    avg = pdv(I, r0, I.perm + r0, 0, v, H, hv);
+                    for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, I.perm + r0, k, v, H, hv));
+                }
+                G.efc[v] = qpart_ef_g(I, r0, v, H, d, avg, P.ef_min);
+            }
+            __syncthreads();
+            return;
+        }
         for (int i = wid; i < nown(); i += kGT / 32) {
             const int v = node(i);
             const int d = deg(v);
@@ -640,7 +658,7 @@ struct GridSolver {
             const int64_t r0 = I.row[v];
             uint16_t* list = I.perm + r0;
             int p = 0;
-            if (scratch && d <= kPartCap) {
+            if (d <= kPartCap) {
                 const double hv = H[v];
                 for (int k = lane; k < d; k += 32) {
                     const uint16_t q = list[k];
