@@ -13,6 +13,14 @@ graph, dual descent, comb extraction and the primal value of every instance.
 Under torchrun each rank solves its own 4,096-instance batch (seed 3 + rank);
 the job time is the max over ranks.  `--impl reference` times the CPU
 restatement of the reference solver (oracle/) on the host cores instead.
+
+On one GPU the line also checks the metric's precision clause: the oracle's
+LP value of every sampled instance (the whole batch by default) against the
+GPU's, exiting with status 3 above 1e-9 relative.  It carries two more
+workloads as sub-objects, each with its own roofline, end-to-end figure, CPU
+baseline and parity check: `large` (one 100,000-point clustered instance,
+N = 50, the grid-wide solver) and `smooth` (smoothed bound + adjoint of 1,024
+jittered-lattice instances, N = 24).
 """
 import argparse
 import json
@@ -34,6 +42,20 @@ METRIC = "batched F2M solves/s vs plain per-instance loop on B200 at LP rel err<
 N_INST = 4096
 TOP_K = 16
 FLUSH_BYTES = 256 << 20
+LP_TOL = 1e-9
+
+# FP64 pipe operations of the persistent solver's Jacobi step, counted from
+# its source (f2m_kernels.cu Solver::step / slice_hgrad / half_grad,
+# f2m_device.cuh top3_insert):
+#   per list entry a warp lane sweeps (padding of the 32-node slices
+#   included): 2 DADD for the reduced cost (D + H[lo]) + H[hi] and 2 DSETP
+#   for the top-3 insertion;
+#   per lane updating a node: 1 DSETP (first value below the 1e6 sentinels),
+#   1 DADD (v1 + v2), 2 DMUL (/2, *0.5) and 1 DADD (H + grad/2).
+# Partitions, gradient checks and comb extraction are not counted, so the
+# fraction is a lower bound.
+FP64_PER_ENTRY = 4
+FP64_PER_LANE = 5
 
 
 def parse():
@@ -53,6 +75,8 @@ def parse():
     ap.add_argument("--n-inst", type=int, default=N_INST)
     ap.add_argument("--plain-sample", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="leave out the large and smooth sub-objects of the batch line")
     ap.add_argument("--size-range", type=int, nargs=2, default=None,
                     help="keep only instances with lo <= points <= hi (profiling one solver class)")
     return ap.parse_args()
@@ -124,15 +148,52 @@ def sample_size(offs, x, y, threads, target_s):
     return int(min(total, max(n, n * target_s / max(dt, 1e-3))))
 
 
-def cpu_baseline(offs, x, y, target_s=15.0):
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def lp_parity(lp_gpu, st_gpu, lp_cpu, st_cpu):
+    """Largest relative LP difference over instances both sides solved, and
+    whether the statuses agree instance by instance."""
+    both = (st_gpu == 0) & (st_cpu == 0)
+    rel = np.abs(lp_gpu[both] - lp_cpu[both]) / np.maximum(np.abs(lp_cpu[both]), 1e-300)
+    return {"max_lp_rel_err_vs_oracle": float(rel.max()) if rel.size else None,
+            "n_checked": int(both.sum()), "status_equal": bool(np.array_equal(st_gpu, st_cpu)),
+            "tolerance": LP_TOL}
+
+
+def cpu_baseline(offs, x, y, lp_gpu=None, st_gpu=None, target_s=15.0):
+    """The oracle on all host threads over a bounded sample of the batch (the
+    whole batch when it fits in target_s), plus one core on a smaller sample.
+    With the GPU's results given, also the LP parity of the sampled instances."""
     threads = cpu_threads()
     n = sample_size(offs, x, y, threads, target_s)
     idx = cpu_sample(offs, n)
     lp, st, dt = run_cpu(offs, x, y, idx, threads)
-    return {"value": len(idx) / dt, "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": f"{len(idx)} instances spread evenly over the batch (same size "
-                      f"distribution), CPU oracle restating the reference solver, "
-                      f"{threads} threads, {dt:.1f} s"}
+    # one core: about 5 s of work, spread over the batch the same way
+    per_inst = dt * threads / len(idx)
+    n1 = int(max(4, min(len(idx), 5.0 / max(per_inst, 1e-6))))
+    idx1 = cpu_sample(offs, n1)
+    _, _, dt1 = run_cpu(offs, x, y, idx1, 1)
+    out = {"value": len(idx) / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+           "cpu_model": cpu_model(),
+           "sample": f"{len(idx)} instances spread evenly over the batch (same size "
+                     f"distribution), CPU oracle restating the reference solver, "
+                     f"{threads} threads, {dt:.1f} s",
+           "one_core": {"value": len(idx1) / dt1, "unit": "solves/s", "cores": 1,
+                        "sample": f"{len(idx1)} instances spread evenly over the batch, "
+                                  f"{dt1:.1f} s"}}
+    parity = None
+    if lp_gpu is not None:
+        parity = lp_parity(np.asarray(lp_gpu)[idx], np.asarray(st_gpu)[idx], lp, st)
+    return out, parity
 
 
 # ---------------------------------------------------------------------------
@@ -236,6 +297,7 @@ def reference_arm(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "config": config(args, world), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "cpu_model": cpu_model(),
                              "sample": f"{len(idx)} instances spread over the batch per step, "
                                        f"CPU restatement of the reference solver (oracle/), "
                                        f"{threads} threads"},
@@ -342,26 +404,44 @@ def ours_arm(args, rank, world, local_rank):
     lp_plain = d_lp.cpu().numpy()[sample]
     plain_err = float(np.max(np.abs(lp_plain - lp[sample]) / np.abs(lp[sample])))
 
+    # FP64 pipe peak of this GPU (the solver's roofline), measured after the
+    # timed region on the same context
+    fp64_dadd = ctx.fp64_rate(0)
+    fp64_dsetp = ctx.fp64_rate(1)
     if rank != 0:
         return
-    # roofline of the dominant kernel: the persistent solver
-    peak, peak_kind = measured_peak()
-    ab = alg_bytes(work)
+    # roofline of the dominant kernel: the persistent solver, bound by the
+    # FP64 pipe (its working set stays in shared memory)
     solve_ms = phase[3]
-    achieved = ab / (solve_ms / 1e3) / 1e9
+    ops = FP64_PER_ENTRY * work["pad_iters"] + FP64_PER_LANE * work["lane_iters"]
+    achieved = ops / (solve_ms / 1e3) / 1e12
+    peak_fp64 = min(fp64_dadd, fp64_dsetp) / 1e12
+    hbm_peak, peak_kind = measured_peak()
+    ab = alg_bytes(work)
     tr = profile_traffic("batch", work)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_job,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)", "config": config(args, world),
-        "roofline": {"bound": "hbm", "kernel": "k_solve (persistent CTA-per-instance solver)",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
+        "roofline": {"bound": "fp64", "kernel": "k_solve (persistent CTA-per-instance solver)",
+                     "achieved": achieved, "peak": peak_fp64, "unit": "T FP64 lane-ops/s",
+                     "frac": achieved / peak_fp64,
+                     "peak_kind": "measured in this run (f2m_fp64_rate: best of 3 launches, "
+                                  "every SM at full occupancy; min of the DADD and DSETP rates)",
+                     "peak_dadd": fp64_dadd / 1e12, "peak_dsetp": fp64_dsetp / 1e12,
+                     "fp64_ops_per_launch": ops,
+                     "fp64_ops_model": f"{FP64_PER_ENTRY} per swept list entry (pad_iters) + "
+                                       f"{FP64_PER_LANE} per node lane (lane_iters), from the source",
+                     "time": "solve phase (CUDA events), all four size classes",
                      "traffic": tr,
-                     "algorithmic_bytes_per_launch": ab,
-                     "note": "active set and potentials stay in SMEM/L1 across iterations; "
-                             "frac > 1 reflects on-chip reuse, traffic is the DRAM bytes"},
+                     "smem_gbs": ab / (solve_ms / 1e3) / 1e9,
+                     "smem_bytes_per_launch": ab,
+                     "hbm_peak_gbs": hbm_peak, "hbm_peak_kind": peak_kind,
+                     "dram_gbs": (tr / (solve_ms / 1e3) / 1e9) if tr else None,
+                     "note": "the active set and potentials stay in shared memory; smem_gbs is "
+                             "the algorithmic byte rate (12 B per active slot + 28 B per node "
+                             "per iteration), served on chip; traffic is the DRAM bytes"},
         "e2e": {"value": n_inst * world / (e2e / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(ho.nbytes + hx.nbytes + hy.nbytes),
                 "d2h_bytes_per_step": int(n_inst * (8 + 4))},
@@ -377,9 +457,188 @@ def ours_arm(args, rank, world, local_rank):
         "iterations_mean": float(work["node_iters"] / max(work["points"], 1)),
         "class_bounds": f2m_b200.get_class_bounds(), "class_bounds_tuned": tuned is not None,
     }
+    bad = False
     if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(offs, x, y)
+        line["cpu_baseline"], line["parity"] = cpu_baseline(offs, x, y, lp, st)
+        p = line["parity"]
+        bad = (p["max_lp_rel_err_vs_oracle"] is None or p["max_lp_rel_err_vs_oracle"] > LP_TOL
+               or not p["status_equal"])
+    if world == 1 and not args.no_sub:
+        ctx.close()
+        line["large"] = large_sub(args, local_rank)
+        line["smooth"] = smooth_sub(args, local_rank)
+        for k in ("large", "smooth"):
+            p = line[k].get("parity") or {}
+            bad |= bool(p.get("fail"))
     print(json.dumps(line), flush=True)
+    if bad:
+        print("parity check failed (LP values differ from the oracle's)", file=sys.stderr)
+        sys.exit(3)
+
+
+def _pool_map(fn, items, threads):
+    """fn over items on `threads` host threads (the oracle releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        return list(ex.map(fn, items))
+
+
+def large_sub(args, local_rank, steps=3, warmup=2):
+    """Sub-object of the batch line: one 100,000-point clustered instance
+    (64 Gaussian clusters, sigma 0.5% of a 10^6 box, 10% uniform background,
+    rounded to integers), N = 50, through f2m_solve_points (host arrays in,
+    full result out), solved by the grid-wide solver.  Roofline of
+    k_solve_grid against the measured HBM copy rate; the oracle on all host
+    threads is its CPU baseline and parity check (LP value, potentials)."""
+    import torch
+
+    import f2m_b200
+    dev = torch.device("cuda", local_rank)
+    x, y = synth.config2(2, n=args.large_n)
+    n_large = 50
+    ctx = f2m_b200.Context(local_rank)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for _ in range(warmup):
+        r = ctx.solve_points(x, y, n_large)
+    clk = Clocks(local_rank)
+    l0 = ctx.kernel_launches()
+    wall, phase = [], np.zeros(4)
+    clk.start()
+    for _ in range(steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = ctx.solve_points(x, y, n_large)
+        wall.append(1e3 * (time.perf_counter() - t0))
+        ph, work = ctx.phase_times()
+        phase += ph
+    clocks = clk.stop()
+    launches = ctx.kernel_launches() - l0
+    ctx.close()
+    phase /= steps
+    dev_ms = float(np.sum(phase))
+    e2e_ms = float(np.mean(wall))
+    peak, peak_kind = measured_peak()
+    ab = alg_bytes(work)
+    achieved = ab / (phase[3] / 1e3) / 1e9
+    out = {
+        "metric": "F2M solves/s, one large clustered instance (device phases)",
+        "value": 1e3 / dev_ms, "unit": "solves/s", "steps": steps, "warmup": warmup,
+        "ms_per_step": dev_ms,
+        "config": {"workload": f"{args.large_n:,} points: 64 Gaussian clusters (sigma 0.5% of a "
+                               "10^6 box) + 10% uniform background, rounded; N=50, reference FP64 "
+                               "Euclidean cost", "top_k": n_large, "seed": 2,
+                   "l2": f"flushed between timed steps ({FLUSH_BYTES >> 20} MiB write)"},
+        "roofline": {"bound": "hbm", "kernel": "k_solve_grid (grid-wide dual descent)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": profile_traffic("large", work),
+                     "algorithmic_bytes_per_launch": ab,
+                     "bytes_model": "12 B per active slot + 28 B per node, per Jacobi iteration",
+                     "time": "solve phase (CUDA events)"},
+        "e2e": {"value": 1e3 / e2e_ms, "unit": "solves/s",
+                "h2d_bytes_per_step": int(x.nbytes + y.nbytes),
+                "d2h_bytes_per_step": int(r.n_edges * 40 + r.n_nodes * 12)},
+        "clocks": clocks, "gpu_launches": int(launches // max(steps, 1)),
+        "phases_ms": {"prep": phase[0], "knn": phase[1], "graph": phase[2], "solve": phase[3],
+                      "host_and_copies": e2e_ms - dev_ms},
+        "work": work, "lp": r.lp, "n_nodes": r.n_nodes, "n_edges": r.n_edges,
+        "iterations": int(r.stats["iterations"]),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        threads = cpu_threads()
+        t0 = time.perf_counter()
+        o = O.solve_points(x, y, n_large, threads=threads)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads,
+                               "kind": "port", "cpu_model": cpu_model(),
+                               "sample": f"the whole instance once, CPU oracle, {threads} threads, "
+                                         f"{dt:.1f} s"}
+        rel = abs(r.lp - o.lp) / abs(o.lp)
+        same_f = bool(o.F is not None and np.array_equal(r.F, o.F))
+        out["parity"] = {"lp_rel_err_vs_oracle": rel, "F_bit_identical": same_f,
+                         "status_equal": r.status == o.status, "tolerance": LP_TOL,
+                         "fail": bool(rel > LP_TOL or not same_f or r.status != o.status)}
+    return out
+
+
+def smooth_sub(args, local_rank, steps=3, warmup=1):
+    """Sub-object of the batch line: smoothed bound + coordinate gradient of
+    1,024 jittered-lattice instances (200-2,000 points, spacing 1, jitter
+    +-0.3, FP32), N = 24, tau = 1e-3, 100 damped Jacobi steps, adjoint with
+    checkpoints every 16 steps; host arrays in and out through the C ABI.
+    The FP64 host oracle on a bounded sample is the CPU baseline and the
+    parity check (bound and gradient)."""
+    import torch
+
+    import f2m_b200
+    offs, x, y = synth.config5(5)
+    N = 24
+    n_inst = len(offs) - 1
+    ctx = f2m_b200.Context(local_rank)
+    p = f2m_b200.default_smooth_params()
+    for _ in range(warmup):
+        ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
+    clk = Clocks(local_rank)
+    l0 = ctx.kernel_launches()
+    ms = []
+    clk.start()
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
+        ms.append(1e3 * (time.perf_counter() - t0))
+    clocks = clk.stop()
+    launches = ctx.kernel_launches() - l0
+    ctx.close()
+    t = float(np.mean(ms))
+    out = {
+        "metric": "smoothed F2M bound + coordinate gradient, instances/s",
+        "value": n_inst / (t / 1e3), "unit": "instances/s", "steps": steps, "warmup": warmup,
+        "ms_per_step": t, "dtype": "f64 (FP32 coordinates)",
+        "config": {"workload": "1,024 instances, sizes uniform in [200,2000], jittered unit "
+                               "lattice (+-0.3), FP32", "top_k": N, "tau": p.tau, "iters": p.iters,
+                   "damping": p.damping, "checkpoint": p.checkpoint, "seed": 5},
+        "e2e": {"value": n_inst / (t / 1e3), "unit": "instances/s",
+                "h2d_bytes_per_step": int(offs.nbytes + x.nbytes + y.nbytes),
+                "d2h_bytes_per_step": int(L.nbytes + gx.nbytes + gy.nbytes)},
+        "clocks": clocks, "gpu_launches": int(launches // max(steps, 1)),
+        "L_mean": float(np.mean(L)),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        threads = cpu_threads()
+
+        def host(b):
+            s_, e_ = offs[b], offs[b + 1]
+            return O.smooth_bound(x[s_:e_], y[s_:e_], N, tau=p.tau, iters=p.iters,
+                                  omega=p.damping, newton_max=p.newton_max, grad=True)
+        # pilot: size the sample for about 10 s of host work
+        pilot = list(range(0, n_inst, max(1, n_inst // (2 * threads))))[: 2 * threads]
+        t0 = time.perf_counter()
+        _pool_map(host, pilot, threads)
+        per = (time.perf_counter() - t0) / len(pilot)
+        n_s = int(min(n_inst, max(len(pilot), 10.0 / max(per, 1e-6))))
+        idx = np.linspace(0, n_inst - 1, n_s).astype(np.int64)
+        t0 = time.perf_counter()
+        res = _pool_map(host, list(idx), threads)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": len(idx) / dt, "unit": "instances/s", "cores": threads,
+                               "kind": "port", "cpu_model": cpu_model(),
+                               "sample": f"{len(idx)} instances spread over the batch, FP64 host "
+                                         f"oracle (bound + adjoint), {threads} threads, {dt:.1f} s"}
+        l_err, g_err = 0.0, 0.0
+        for b, (Lo, dx, dy, _) in zip(idx, res):
+            s_, e_ = offs[b], offs[b + 1]
+            l_err = max(l_err, abs(L[b] - Lo) / abs(Lo))
+            scale = max(np.abs(dx).max(), np.abs(dy).max(), 1e-300)
+            g_err = max(g_err, float(max(np.abs(gx[s_:e_] - dx).max(),
+                                         np.abs(gy[s_:e_] - dy).max()) / scale))
+        out["parity"] = {"n_checked": len(idx), "max_L_rel_err_vs_oracle": l_err,
+                         "max_grad_err_rel_to_max": g_err,
+                         "tolerance": {"L": 1e-9, "grad": 1e-5},
+                         "fail": bool(l_err > 1e-9 or g_err > 1e-5)}
+    return out
 
 
 def large_arm(args, rank, world, local_rank):

@@ -46,7 +46,7 @@ class Params(ctypes.Structure):
         ("ef_min", ctypes.c_int32), ("comb_thr", ctypes.c_double),
         ("shift0", ctypes.c_double), ("shift_max", ctypes.c_double),
         ("max_iters", ctypes.c_int64), ("cost_mode", ctypes.c_int32),
-        ("solver", ctypes.c_int32),
+        ("solver", ctypes.c_int32), ("grid_spin_limit", ctypes.c_int64),
     ]
 
 
@@ -65,7 +65,8 @@ class Stats(ctypes.Structure):
 
 class Work(ctypes.Structure):
     _fields_ = [("node_iters", ctypes.c_int64), ("slot_iters", ctypes.c_int64),
-                ("slots", ctypes.c_int64), ("points", ctypes.c_int64)]
+                ("slots", ctypes.c_int64), ("points", ctypes.c_int64),
+                ("pad_iters", ctypes.c_int64), ("lane_iters", ctypes.c_int64)]
 
 
 class BatchOut(ctypes.Structure):
@@ -90,7 +91,8 @@ EXPORTS = [
     "f2m_result_edges", "f2m_result_nodes", "f2m_result_stats", "f2m_phase_times",
     "f2m_solve_points_noalloc", "f2m_default_smooth_params", "f2m_smoothed_bound_fwd",
     "f2m_smoothed_bound_bwd", "f2m_smooth_max_nodes", "f2m_knn", "f2m_set_class_bounds",
-    "f2m_get_class_bounds", "f2m_solve_graph", "f2m_solve_points_from",
+    "f2m_get_class_bounds", "f2m_solve_graph", "f2m_solve_points_from", "f2m_fp64_rate",
+    "f2m_smoothed_bound_bwd_edges",
 ]
 
 _lib = None
@@ -132,11 +134,14 @@ def lib():
         L.f2m_result_nodes.argtypes = [vp] * 3
         L.f2m_result_stats.argtypes = [vp, P(Stats)]
         L.f2m_phase_times.argtypes = [vp, vp, P(Work)]
+        L.f2m_fp64_rate.argtypes = [vp, i32, i32, P(dbl)]
         L.f2m_solve_points_noalloc.argtypes = [vp, vp, i32, i32, P(Params), vp, vp, vp]
         L.f2m_default_smooth_params.argtypes = [P(SmoothParams)]
         L.f2m_smoothed_bound_fwd.argtypes = [vp, i32, vp, vp, vp, i32, P(SmoothParams), vp]
         L.f2m_smoothed_bound_bwd.argtypes = [vp, i32, vp, vp, vp, i32, P(SmoothParams), vp, vp,
                                              vp, vp]
+        L.f2m_smoothed_bound_bwd_edges.argtypes = [vp, i32, vp, vp, vp, i32, P(SmoothParams), vp,
+                                                   vp, vp, vp, i64, P(i64), vp, vp, vp, vp]
         L.f2m_smooth_max_nodes.restype = i32
         L.f2m_set_class_bounds.argtypes = [vp]
         L.f2m_get_class_bounds.argtypes = [vp]
@@ -273,6 +278,13 @@ class Context:
         self._check(lib().f2m_phase_times(self._h, _ptr(ms), ctypes.byref(w)))
         return ms, {k: getattr(w, k) for k, _ in Work._fields_}
 
+    def fp64_rate(self, kind=0, repeats=3):
+        """Measured FP64 pipe rate of this GPU, FP64 lane operations per second
+        (kind 0: DADD, kind 1: DSETP); the roofline of the dual descent."""
+        r = ctypes.c_double()
+        self._check(lib().f2m_fp64_rate(self._h, kind, repeats, ctypes.byref(r)))
+        return r.value
+
     # -- single instance ----------------------------------------------------
     # -- smoothed bound (no counterpart in the reference) ------------------
     def smoothed_bound(self, offs, x, y, top_k, params=None, grad=False, dL=None):
@@ -295,6 +307,31 @@ class Context:
                                                  ctypes.byref(p), _ptr(up), _ptr(L), _ptr(gx),
                                                  _ptr(gy)))
         return L, gx, gy
+
+    def smoothed_bound_edges(self, offs, x, y, top_k, params=None, dL=None):
+        """Backward with the edge-cost gradient: returns (L, dL_dx, dL_dy, edges)
+        where edges = (a, b, c, dL_dc): each edge once (a < b, global point
+        indices), its FP32 cost and d(sum_b dL[b] L[b]) / dc_e."""
+        offs = np.ascontiguousarray(offs, np.int64)
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        n = len(offs) - 1
+        p = params if params is not None else default_smooth_params()
+        L = np.zeros(n, np.float64)
+        gx = np.zeros(len(x), np.float32)
+        gy = np.zeros(len(y), np.float32)
+        cap = len(x) * int(top_k)
+        a = np.zeros(cap, np.int32)
+        b = np.zeros(cap, np.int32)
+        c = np.zeros(cap, np.float32)
+        dc = np.zeros(cap, np.float64)
+        m = ctypes.c_int64()
+        up = None if dL is None else np.ascontiguousarray(dL, np.float64)
+        self._check(lib().f2m_smoothed_bound_bwd_edges(
+            self._h, n, _ptr(offs), _ptr(x), _ptr(y), top_k, ctypes.byref(p), _ptr(up), _ptr(L),
+            _ptr(gx), _ptr(gy), cap, ctypes.byref(m), _ptr(a), _ptr(b), _ptr(c), _ptr(dc)))
+        k = m.value
+        return L, gx, gy, (a[:k], b[:k], c[:k], dc[:k])
 
     def solve_graph(self, n_nodes, v1, v2, D, Do, labels=None, params=None):
         """graph_c + RUN on a caller-built graph (edges in the reference's order)."""

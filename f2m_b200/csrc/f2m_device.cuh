@@ -152,11 +152,15 @@ __device__ __forceinline__ double red_d(const Slot& s, int v, HP H, double hv) {
 
 // Sorted insertion of x into (v0 <= v1 <= v2) keeping the three smallest:
 // the reference's compare chain (strict <, so ties and NaN leave the triple
-// as it is) written as three compares and selects.  The selects run on the
-// integer pipe; the FP64 pipe, which bounds the dual step on this GPU, only
-// sees the compares.
+// as it is) written as two FP64 compares and integer selects.  x < v1 decides
+// the half: if it holds, x < v2 holds too and only x < v0 is open; if not,
+// x < v0 fails too and only x < v2 is open.  One select picks the bound of
+// the open compare.  The selects run on the integer pipe; the FP64 pipe,
+// which bounds the dual step on this GPU, sees two compares per entry.
 __device__ __forceinline__ void top3_insert(double x, double& v0, double& v1, double& v2) {
-    const bool c0 = x < v0, c1 = x < v1, c2 = x < v2;
+    const bool c1 = x < v1;
+    const bool cy = x < (c1 ? v0 : v2);
+    const bool c0 = c1 && cy, c2 = c1 || cy;
     v2 = c1 ? v1 : (c2 ? x : v2);
     v1 = c0 ? v0 : (c1 ? x : v1);
     v0 = c0 ? x : v0;
@@ -248,6 +252,65 @@ static __device__ int qpart_ef(const Inst& I, int64_t r0, int v, HP H, int size,
         bump_until(avg, bump, g, kLimit);
     }
     return size;
+}
+
+/* ------------------------------------------------------------------ */
+/* Ax=b of an irregular comb                                            */
+/* ------------------------------------------------------------------ */
+// The linear system of one comb (comb::solve_AxB, comb_thread.cpp:272-304):
+// a row per comb node whose entries (coefficient 1) are the node's B edges
+// (|d| < porog over its whole list, node.cpp:49-57) and whose right-hand side
+// is 2 minus its A edges (d <= -porog); the variables are the B edges,
+// numbered on first sight.  CSR: row k's variables are col[rs[k] .. rs[k+1]).
+struct AxbRows {
+    int m, z, q;  // rows, entries, variables
+    const int* rs;
+    const int* col;
+    const int* rhs;
+};
+
+// Doubles of scratch an Ax=b system of m rows and z entries needs: ints rs
+// (m+1), col (z), rhs (m), the variables' edge slots (<= z); doubles Aj, d,
+// b_grad (m each), x, x_grad (<= z each).
+__device__ __forceinline__ long long axb_scratch_doubles(long long m, long long z) {
+    return 3 * m + 2 * z + (2 * m + 2 * z + 1 + 1) / 2 + 2;
+}
+
+// Ax_b::solve (Ax_b.cpp:87-158) by one thread: steepest descent on the
+// row-scaled residual with an exact line search, until the largest scaled
+// residual is below 1e-8 (at most 999 steps).  FP64 in the reference's
+// operation order within each row and over the rows, without multiply-add
+// contraction (the reference's host code has none).  Returns the step count
+// at convergence, 0 when it did not converge (Ax_b::go_max).
+static __device__ __noinline__ int axb_solve(const AxbRows& S, double* Aj, double* d, double* bg, double* x,
+                                      double* xg) {
+    for (int j = 0; j < S.m; ++j) Aj[j] = sqrt((double)(S.rs[j + 1] - S.rs[j]));
+    for (int i = 0; i < S.q; ++i) x[i] = 0.0;
+    for (int go = 1; go < 1000; ++go) {
+        for (int i = 0; i < S.q; ++i) xg[i] = 0.0;
+        double dmax = 0.0;
+        for (int j = 0; j < S.m; ++j) {
+            double ax = 0.0;
+            for (int k = S.rs[j]; k < S.rs[j + 1]; ++k) ax = __dadd_rn(ax, x[S.col[k]]);
+            const double dj = __dsub_rn(ax, (double)S.rhs[j]) / Aj[j];
+            d[j] = dj;
+            if (fabs(dj) > dmax) dmax = fabs(dj);
+            const double gj = dj / Aj[j];
+            for (int k = S.rs[j]; k < S.rs[j + 1]; ++k) xg[S.col[k]] = __dadd_rn(xg[S.col[k]], gj);
+        }
+        if (dmax < 1e-8) return go;
+        double gg = 0.0, gd = 0.0;
+        for (int j = 0; j < S.m; ++j) {
+            double bj = 0.0;
+            for (int k = S.rs[j]; k < S.rs[j + 1]; ++k) bj = __dadd_rn(bj, xg[S.col[k]]);
+            bg[j] = bj;
+        }
+        for (int j = 0; j < S.m; ++j) gg = __dadd_rn(gg, __dmul_rn(bg[j], bg[j]));
+        for (int j = 0; j < S.m; ++j) gd = __dadd_rn(gd, __dmul_rn(d[j], bg[j]));
+        const double alfa = -gd / gg;
+        for (int i = 0; i < S.q; ++i) x[i] = __dadd_rn(x[i], __dmul_rn(xg[i], alfa));
+    }
+    return 0;
 }
 
 }  // namespace f2m

@@ -31,7 +31,6 @@
 namespace f2m {
 
 constexpr int kGT = 1024;              // threads per CTA (one CTA per SM: fewer barrier arrivals)
-constexpr long long kSpinLimit = 1LL << 26;  // ~seconds of waiting before giving up
 constexpr int kMaxBlk = 16;            // most Jacobi steps between two grid barriers
 constexpr int kMaxNl = 2048;           // most nodes in a CTA's halo
 constexpr unsigned long long kHEmpty = ~0ull;
@@ -332,7 +331,7 @@ struct GridSolver {
                 } else {
                     for (long long spins = 1; ld_acquire_u32(gen) == g; ++spins) {
                         if ((spins & 63) == 0 && (bad = ld_acquire_i32(G.err)) != 0) break;
-                        if (spins > kSpinLimit) { atomicExch(G.err, 1); bad = 1; break; }
+                        if (spins > P.spin_limit) { atomicExch(G.err, 1); bad = 1; break; }
                     }
                 }
             }
@@ -840,6 +839,7 @@ struct GridSolver {
         const long long wsum = gsum_ll(wslots);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             B.work_slots[b] = (accumulate ? B.work_slots[b] : 0) + wsum;
+            B.work_pad[b] = (accumulate ? B.work_pad[b] : 0) + wsum;
             const double dmin = __longlong_as_double((long long)B.dmin_bits[b]);
             B.n_edges[b] = (int32_t)((I.row[V] - I.row[0]) / 2);
             B.n_combs[b] = (int32_t)nc;

@@ -32,6 +32,7 @@ struct DevParams {
     int32_t fix_rounds, fix_factor, check_every, frozen_iters;
     int32_t ef_small_deg, ef_min;
     int64_t max_iters;
+    int64_t spin_limit;     // grid barrier polls before giving up (whole-GPU solver)
 };
 
 // Pointers of one batched call.  Node g of instance b lives at index
@@ -89,7 +90,8 @@ struct Batch {
     int32_t* mirror;        // [S] position of the same edge in the neighbour's list
     double* efD;            // [S] active-set arena (update_EF copies): D
     uint16_t* efN;          // [S] active-set arena: neighbour
-    uint8_t* xcode;         // [S] 0, 1 (= 1/2), 2 (= 1)
+    uint8_t* xcode;         // [S] 0, 1 (= 1/2), 2 (= 1), 3 (= xval: an Ax=b solution)
+    float* xval;            // [S] x of the B edges of combs solved by Ax=b on the device
     double* selD;           // [S] SELL-32 slices that do not fit in shared memory: D
     uint16_t* selW;         // [S] ... neighbour word; instance b owns sel_stride * offs[b] ..
     int64_t sel_stride;     //     sel_stride * offs[b+1] (S / n_total entries per point)
@@ -110,6 +112,7 @@ struct Batch {
     int64_t* iters;
     int64_t* work_nodes;    // sum over Jacobi iterations of V
     int64_t* work_slots;    // sum over Jacobi iterations of active slots
+    int64_t* work_pad;      // sum over Jacobi iterations of the entries swept incl. SELL padding
     int32_t* checks;
     double* max_grad;
     double* dual;
@@ -169,6 +172,9 @@ size_t edge_order_temp_bytes(int64_t S);
 // S/2 entries of *order are the edges in order.
 cudaError_t launch_edge_order(const Batch& B, int b, int V, int64_t S, const EdgeSort& E, const uint32_t** order,
                               cudaStream_t s, int64_t* launches);
+// FP64 pipe throughput probe (f2m_probe.cu): kind 0 DADD chains, kind 1 DSETP.
+cudaError_t launch_fp64_probe(int kind, int blocks, int iters, double* out, cudaStream_t s);
+double fp64_probe_ops(int kind, int blocks, int iters);
 cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches);
 cudaError_t launch_knn(const Batch& B, int64_t* scan_scratch, cudaStream_t s, int64_t* launches);
 cudaError_t launch_graph(const Batch& B, int64_t* deg_scratch, int64_t* scan_scratch,

@@ -793,7 +793,8 @@ struct TeamMem {
     uint16_t* ord;   // 32*NS: nodes in slice order
     int* soff;       // NS: >= 0 shared offset; kSelGlobal + g: global offset g; kSelNode: node copy
     int* swid;       // NS: slice width (longest list)
-    int* hist;       // 257: counting-sort buckets; hist[256] = total list length
+    int* hist;       // 258: counting-sort buckets; hist[256] = total list length,
+                     // hist[257] = SELL entries incl. padding (32 x slice width, summed)
     double* eD;      // cap entries: D
     uint16_t* eW;    // cap entries: neighbour | 0x8000 when the neighbour is the lower id
     double* gsD;     // gcap entries in global memory
@@ -817,7 +818,7 @@ __device__ __forceinline__ TeamMem carve_team(unsigned char* base, size_t bytes,
     M.Hb = reinterpret_cast<double*>(base + o); o = align16(o + (size_t)V * 8);
     M.soff = reinterpret_cast<int*>(base + o); o = align16(o + (size_t)M.NS * 4);
     M.swid = reinterpret_cast<int*>(base + o); o = align16(o + (size_t)M.NS * 4);
-    M.hist = reinterpret_cast<int*>(base + o); o = align16(o + 257 * 4);
+    M.hist = reinterpret_cast<int*>(base + o); o = align16(o + 258 * 4);
     M.ord = reinterpret_cast<uint16_t*>(base + o); o = align16(o + (size_t)M.NS * 32 * 2);
     M.eD = reinterpret_cast<double*>(base + o);
     const long long rest = (long long)bytes - (long long)o;
@@ -835,7 +836,7 @@ __device__ __forceinline__ TeamMem carve_team(unsigned char* base, size_t bytes,
 }
 __device__ __host__ inline size_t team_fixed_bytes(int V) {
     const int NS = (V + 31) / 32;
-    return (size_t)V * 16 + (size_t)NS * 8 + 257 * 4 + (size_t)NS * 64 + 5 * 16;
+    return (size_t)V * 16 + (size_t)NS * 8 + 258 * 4 + (size_t)NS * 64 + 5 * 16;
 }
 
 __device__ __forceinline__ uint16_t ef_word(int v, int nbr) {
@@ -871,6 +872,81 @@ __device__ __forceinline__ double half_grad(int n, Get get) {
     return (-(v1 + v2) / 2) * 0.5;
 }
 
+// One irregular comb's Ax=b, built and solved by one thread (the body of
+// Solver::axb_irregular, out of line to keep the solver's registers free).
+// The rows are the comb's nodes (lab[u] == r) in ascending id; the system
+// goes to the scratch at *w, which advances past it.  Writes x (FP32) of
+// the comb's B edges whose larger-root comb is this one to both slots of
+// the edge.  Returns 1 when the system did not converge within 900 steps
+// or a slot has no twin.
+__device__ __noinline__ int axb_comb(const Slot* slot, const int64_t* row, int64_t row0, const int32_t* mirror,
+                                     const double* H, const int* lab, int V, int r, double porog,
+                                     double** wp, float* xval) {
+    int m = 0, z = 0;
+    for (int u = 0; u < V; ++u) {
+        if (lab[u] != r) continue;
+        m++;
+        const double hu = H[u];
+        for (int64_t a = row[u]; a < row[u + 1]; ++a) {
+            const double d = red_d(slot[a], u, H, hu);
+            if (d < porog && d > -porog) z++;
+        }
+    }
+    double* w = *wp;
+    *wp = w + axb_scratch_doubles(m, z);
+    int* rs = reinterpret_cast<int*>(w);
+    int* col = rs + m + 1;
+    int* rhs = col + z;
+    int* vs = rhs + m;  // canonical slot (offset in the instance) of each variable
+    double* Aj = w + (2 * m + 2 * z + 2) / 2;
+    double* dd = Aj + m;
+    double* bg = dd + m;
+    double* x = bg + m;
+    double* xg = x + z;
+    int j = 0, k = 0, q = 0;
+    for (int u = 0; u < V; ++u) {
+        if (lab[u] != r) continue;
+        const double hu = H[u];
+        int na = 0;
+        rs[j] = k;
+        for (int64_t a = row[u]; a < row[u + 1]; ++a) {
+            const Slot s = slot[a];
+            const double d = red_d(s, u, H, hu);
+            if (!(d < porog)) continue;
+            if (!(d > -porog)) { na++; continue; }
+            const int mi = mirror[a];
+            if (mi < 0) return 1;
+            const int cs = (int)((s.nbr > u ? a : row[s.nbr] + mi) - row0);
+            int t = 0;
+            while (t < q && vs[t] != cs) ++t;
+            if (t == q) vs[q++] = cs;
+            col[k++] = t;
+        }
+        rhs[j++] = 2 - na;
+    }
+    rs[m] = k;
+    const AxbRows S{m, z, q, rs, col, rhs};
+    const int go = axb_solve(S, Aj, dd, bg, x, xg);
+    if (go == 0 || go > 900) return 1;
+    k = 0;
+    for (int u = 0; u < V; ++u) {
+        if (lab[u] != r) continue;
+        const double hu = H[u];
+        for (int64_t a = row[u]; a < row[u + 1]; ++a) {
+            const Slot s = slot[a];
+            const double d = red_d(s, u, H, hu);
+            if (!(d < porog) || !(d > -porog)) continue;
+            const int t = col[k++];
+            const int ln = lab[s.nbr];
+            if (ln != INT_MAX && ln > r) continue;  // the neighbour's comb decides
+            const float xv = (float)x[t];
+            xval[a] = xv;
+            xval[row[s.nbr] + mirror[a]] = xv;
+        }
+    }
+    return 0;
+}
+
 template <int TEAM>
 struct Solver {
     static constexpr int WARPS = TEAM / 32;
@@ -883,7 +959,8 @@ struct Solver {
     double* Hn;   // next (Jacobi double buffer)
     int64_t row0;
     long long iters = 0;
-    long long wslots = 0;  // active slots read, summed over iterations (warp leaders)
+    long long wslots = 0;  // active slots read, summed over iterations
+    long long wpad = 0;    // SELL entries the warps sweep (padding included), summed over iterations
     int checks = 0;
     bool capped = false;
 
@@ -926,6 +1003,7 @@ struct Solver {
             if (v >= 0) Hn[v] = (MASKED && B.shift[I.base + v] != 0.0) ? Hc[v] : Hc[v] + g;
         }
         wslots += M.hist[256];
+        wpad += M.hist[257];
         T.sync();
         swap_f();
         iters++;
@@ -1002,6 +1080,7 @@ struct Solver {
             }
             carry += t;
         }
+        if (T.tid == 0) M.hist[257] = carry;  // read after the barriers below
         lead = T.max_ll(lead);
         for (int s = T.tid; s < M.NS; s += TEAM) {
             const int pos = M.soff[s], size = 32 * M.swid[s];
@@ -1099,6 +1178,57 @@ struct Solver {
         }
         return M_;
     }
+    // B edges (|d| < porog) of node u over its whole list; *nA = its A edges
+    // (d <= -porog), the host's classification (node::get_statusAB,
+    // node.cpp:49-57)
+    __device__ int count_ab(int u, double porog, int* nA) const {
+        const double hu = Hc[u];
+        int nb = 0, na = 0;
+        for (int64_t a = I.row[u]; a < I.row[u + 1]; ++a) {
+            const double d = red_d(I.slot[a], u, Hc, hu);
+            if (d < porog) { if (d > -porog) nb++; else na++; }
+        }
+        *nA = na;
+        return nb;
+    }
+    // comb::solve_AxB (comb_thread.cpp:272-304) for every irregular comb of
+    // the instance, on the device: a thread per comb (roots r = tid, tid +
+    // TEAM, ...), its system in the instance's part of the global slice arena
+    // (free once the descent is over).  The rows are the comb's nodes in
+    // ascending id (the reference takes them in its hash map's order; the
+    // solution does not depend on the order, its last bits may).  Each B edge
+    // takes x (as FP32, as comb::XB holds it) from the comb the host applies
+    // last: graph::X is filled comb by comb in root order, so the comb with
+    // the larger root of the edge's two ends.  Returns false -- the instance
+    // then goes to the host stage, which also runs the repair loop
+    // (graph_cuda.cu:69-126) -- when a system does not converge within 900
+    // steps (the reference allows 999: near that limit the order could
+    // decide) or the arena cannot hold the systems.
+    __device__ bool axb_irregular(const int* irr, const int* lab, double porog) {
+        const int V = I.V;
+        long long need = 0;
+        for (int r = T.tid; r < V; r += TEAM) {
+            if (lab[r] != r || !irr[r]) continue;
+            long long m = 0, z = 0;
+            for (int u = 0; u < V; ++u) {
+                if (lab[u] != r) continue;
+                int na;
+                m++;
+                z += count_ab(u, porog, &na);
+            }
+            need += axb_scratch_doubles(m, z);
+        }
+        int total = 0;  // (a thread's share is clamped so that the team sum fits an int)
+        const int off = T.excl_scan((int)::min(need, (long long)1 << 20), &total);
+        if (total > M.gcap) return false;  // team-uniform
+        int bad = need >= ((long long)1 << 20) ? 1 : 0;
+        double* w = M.gsD + off;
+        for (int r = T.tid; r < V && !bad; r += TEAM) {
+            if (lab[r] != r || !irr[r]) continue;
+            bad = axb_comb(I.slot, I.row, row0, B.mirror, Hc, lab, V, r, porog, &w, B.xval);
+        }
+        return T.sum_ll(bad) == 0;
+    }
     // Comb extraction (graph_cuda_comb.hpp:415-475), the device comb check and
     // the primal; writes the per-node state for the host and the results.
     __device__ void combs_and_primal(int b, double M_, bool accumulate) {
@@ -1169,8 +1299,12 @@ struct Solver {
             if (lab[v] == v) { nc++; ni += irr[v]; }
         nc = T.sum_ll(nc);
         ni = T.sum_ll(ni);
+        // irregular combs: Ax=b on the device (the first solve only; after a
+        // repair shift the host driver runs the comb stage itself)
+        const bool solved = (ni == 0) || (!accumulate && axb_irregular(irr, lab, porog));
         // primal (graph_cuda.cu:135-147): x = 1 on A edges, 1/2 on the B edges
-        // of regular combs; OVAL = sum x*Do, MAX edge rank (graph_tour.hpp:165-184)
+        // of regular combs, the Ax=b solution on those of irregular ones;
+        // OVAL = sum x*Do, MAX edge rank (graph_tour.hpp:165-184)
         double lp = 0.0, dual_neg = 0.0, fsum = 0.0;
         long long maxr = -1, viol = 0;
         for (int v = T.tid; v < V; v += TEAM) {
@@ -1182,14 +1316,21 @@ struct Solver {
             for (int64_t a = r0; a < r1; ++a) {
                 const Slot s = I.slot[a];
                 const double d = red_d(s, v, Hc, hv);
-                const double x = (d < porog) ? ((d > -porog) ? 0.5 : 1.0) : 0.0;
-                B.xcode[a] = (uint8_t)(x == 1.0 ? 2 : (x == 0.5 ? 1 : 0));
+                double x = (d < porog) ? ((d > -porog) ? 0.5 : 1.0) : 0.0;
+                uint8_t code = (uint8_t)(x == 1.0 ? 2 : (x == 0.5 ? 1 : 0));
+                if (ni > 0 && solved && code == 1) {
+                    const int l1 = lab[v], l2 = lab[s.nbr];
+                    const int c = (l2 == INT_MAX) ? l1 : (l1 == INT_MAX ? l2 : ::max(l1, l2));
+                    if (c != INT_MAX && irr[c]) { x = (double)B.xval[a]; code = 3; }
+                }
+                B.xcode[a] = code;
+                const bool in_x = (x != 0.0) || code == 3;  // every comb edge enters graph::X
                 degsum += (float)x;
-                any |= (x != 0.0);
+                any |= in_x;
                 if (s.nbr > v) {
                     lp += x * B.s_cost[a];
                     dual_neg += fmin(0.0, d);
-                    if (x != 0.0) maxr = ::max(maxr, (long long)::min((int)(a - r0), B.mirror[a]));
+                    if (in_x) maxr = ::max(maxr, (long long)::min((int)(a - r0), B.mirror[a]));
                 }
             }
             if (any && !(degsum > 2.0f - 1e-2f && degsum < 2.0f + 1e-2f)) viol++;
@@ -1209,11 +1350,12 @@ struct Solver {
             B.iters[b] = (accumulate ? B.iters[b] : 0) + iters;
             B.work_nodes[b] = (accumulate ? B.work_nodes[b] : 0) + iters * (long long)V;
             B.work_slots[b] = (accumulate ? B.work_slots[b] : 0) + wslots;
+            B.work_pad[b] = (accumulate ? B.work_pad[b] : 0) + wpad;
             B.checks[b] = (accumulate ? B.checks[b] : 0) + checks;
             B.max_grad[b] = M_;
             B.dual[b] = dmin * (-fsum + dual_neg);
             if (capped) { B.status[b] = F2M_ERR_NOT_CONVERGED; B.lp[b] = NAN; }
-            else if (ni > 0) { B.status[b] = kNeedsHost; B.lp[b] = NAN; }
+            else if (!solved) { B.status[b] = kNeedsHost; B.lp[b] = NAN; }
             else { B.status[b] = F2M_OK; B.lp[b] = lp; }
         }
         T.sync();

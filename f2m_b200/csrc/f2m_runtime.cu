@@ -137,6 +137,7 @@ DevParams to_dev(const f2m_params& p) {
     d.ef_small_deg = p.ef_small_deg;
     d.ef_min = p.ef_min;
     d.max_iters = p.max_iters;
+    d.spin_limit = p.grid_spin_limit > 0 ? p.grid_spin_limit : 1;
     return d;
 }
 
@@ -274,6 +275,7 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.efD = A.take<double>(S);
     B.efN = A.take<uint16_t>(S);
     B.xcode = A.take<uint8_t>(S);
+    B.xval = A.take<float>(S);
     B.selD = A.take<double>(S);
     B.selW = A.take<uint16_t>(S);
     B.sel_stride = S / n;
@@ -291,6 +293,7 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.iters = A.take<int64_t>(ni);
     B.work_nodes = A.take<int64_t>(ni);
     B.work_slots = A.take<int64_t>(ni);
+    B.work_pad = A.take<int64_t>(ni);
     B.checks = A.take<int32_t>(ni);
     B.max_grad = A.take<double>(ni);
     B.dual = A.take<double>(ni);
@@ -1087,24 +1090,33 @@ f2m_status complete_from_device(f2m_ctx* ctx, const DevCall& C, int b, f2m_resul
     Range rg("f2m complete instance (device combs)");
     HostInst& H = R.H;
     int64_t base = 0, s0 = 0;
-    int32_t nc = 0;
+    int32_t nc = 0, ni = 0;
     F2M_CUDA(cudaMemcpyAsync(&base, C.B.offs + b, sizeof(base), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
     F2M_CUDA(cudaMemcpyAsync(&s0, C.B.row + base, sizeof(s0), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaMemcpyAsync(&nc, C.B.n_combs + b, sizeof(nc), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaMemcpyAsync(&ni, C.B.n_irr + b, sizeof(ni), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
     const int64_t S = (int64_t)H.nbr.size();
-    F2M_CUDA(ensure_pinned(ctx, (size_t)std::max<int64_t>(S, 1)));
+    // per-slot codes, and the Ax=b values where the device solved irregular combs
+    const size_t xv_off = ((size_t)S + 15) & ~(size_t)15;
+    F2M_CUDA(ensure_pinned(ctx, xv_off + (ni > 0 ? (size_t)S * sizeof(float) : 0) + 16));
     F2M_CUDA(cudaMemcpyAsync(ctx->pinned, C.B.xcode + s0, S, cudaMemcpyDeviceToHost, ctx->stream));
+    if (ni > 0)
+        F2M_CUDA(cudaMemcpyAsync(ctx->pinned + xv_off, C.B.xval + s0, S * sizeof(float), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
     const uint8_t* xc = reinterpret_cast<const uint8_t*>(ctx->pinned);
+    const float* xv = reinterpret_cast<const float*>(ctx->pinned + xv_off);
     R.x.assign(H.E, 0.0);
+    std::vector<char> inx(H.E, 0);  // in graph::X (every comb edge is, whatever its value)
     parallel_for(H.E, [&](int64_t e0, int64_t e1) {
         for (int64_t e = e0; e < e1; ++e) {
             const int v = H.ev1[e];
             const int64_t a = H.row[v] + (H.el1[e] == v ? H.rank1[e] : H.rank2[e]);
             const uint8_t c = xc[a];
-            R.x[e] = c == 2 ? 1.0 : (c == 1 ? 0.5 : 0.0);
+            R.x[e] = c == 3 ? (double)xv[a] : (c == 2 ? 1.0 : (c == 1 ? 0.5 : 0.0));
+            inx[e] = c != 0;
         }
     });
     R.X.clear();
@@ -1114,7 +1126,7 @@ f2m_status complete_from_device(f2m_ctx* ctx, const DevCall& C, int b, f2m_resul
     std::vector<char> has(H.V, 0);
     for (int e = 0; e < H.E; ++e) {
         const double x = R.x[e];
-        if (x == 0.0) continue;
+        if (!inx[e]) continue;
         R.X.emplace(e, x);
         mr = std::max(mr, std::min(H.rank1[e], H.rank2[e]));
         OVAL += x * H.eDo[e];
@@ -1128,7 +1140,7 @@ f2m_status complete_from_device(f2m_ctx* ctx, const DevCall& C, int b, f2m_resul
     R.max_rank = mr;
     R.status = F2M_OK;
     R.st.repair_steps = 0;
-    R.st.irr_a = 0;
+    R.st.irr_a = ni;  // irregular combs, solved by Ax=b on the device
     R.st.irr_b = 0;
     R.st.n_combs = nc;
     R.st.degree_violations = viol;
@@ -1188,6 +1200,7 @@ void f2m_default_params(f2m_params* p) {
     p->max_iters = 20000000;
     p->cost_mode = F2M_COST_REF_EUCLID;
     p->solver = 0;
+    p->grid_spin_limit = (int64_t)1 << 26;
 }
 
 f2m_status f2m_create(f2m_ctx** out, int device) {
@@ -1250,17 +1263,23 @@ f2m_status f2m_phase_times(f2m_ctx* ctx, float* ms, f2m_work* work) {
     if (work) {
         const Batch& B = ctx->last;
         const int n = B.n_inst;
-        std::vector<int64_t> wn(n), ws(n);
+        std::vector<int64_t> wn(n), ws(n), wp(n), it(n);
         std::vector<int32_t> vn(n), st(n);
         int64_t slots = 0;
         F2M_CUDA(cudaMemcpy(wn.data(), B.work_nodes, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
         F2M_CUDA(cudaMemcpy(ws.data(), B.work_slots, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(wp.data(), B.work_pad, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(it.data(), B.iters, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
         F2M_CUDA(cudaMemcpy(vn.data(), B.Vn, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(st.data(), B.status, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
         F2M_CUDA(cudaMemcpy(&slots, B.row + B.n_total, sizeof(int64_t), cudaMemcpyDeviceToHost));
-        *work = f2m_work{0, 0, slots, 0};
+        *work = f2m_work{0, 0, slots, 0, 0, 0};
         for (int b = 0; b < n; ++b) {
+            if (st[b] == F2M_ERR_INPUT || st[b] == F2M_ERR_CAPACITY) continue;  // never solved
             work->node_iters += wn[b];
             work->slot_iters += ws[b];
+            work->pad_iters += wp[b];
+            work->lane_iters += it[b] * 32 * (int64_t)((vn[b] + 31) / 32);
             work->points += vn[b];
         }
     }
@@ -1272,6 +1291,32 @@ int64_t f2m_kernel_launches(const f2m_ctx* c) { return c ? c->launches : 0; }
 
 f2m_status f2m_sync(f2m_ctx* ctx) {
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    return F2M_OK;
+}
+
+f2m_status f2m_fp64_rate(f2m_ctx* ctx, int32_t kind, int32_t repeats, double* lane_ops_per_s) {
+    if (!ctx || !lane_ops_per_s || (kind != 0 && kind != 1) || repeats < 1)
+        return fail(ctx, F2M_ERR_INPUT, "f2m_fp64_rate: kind 0 or 1, repeats >= 1");
+    F2M_CUDA(cudaSetDevice(ctx->device));
+    int per_sm = 0;
+    F2M_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxThreadsPerMultiProcessor, ctx->device));
+    const int blocks = ctx->sms * (per_sm / 256);  // full occupancy of 256-thread CTAs
+    constexpr int kIters = 40000;
+    F2M_CUDA(ensure_device(ctx, 4096));
+    double* out = reinterpret_cast<double*>(ctx->dev);
+    double best = 0.0;
+    for (int r = 0; r <= repeats; ++r) {  // the first launch warms up
+        F2M_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+        F2M_CUDA(launch_fp64_probe(kind, blocks, kIters, out, ctx->stream));
+        F2M_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+        F2M_CUDA(cudaEventSynchronize(ctx->ev[1]));
+        ctx->launches++;
+        float ms = 0.f;
+        F2M_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+        if (r > 0 && ms > 0.f) best = std::max(best, fp64_probe_ops(kind, blocks, kIters) / (ms * 1e-3));
+    }
+    ctx->timed = false;  // the phase events now hold the probe's times
+    *lane_ops_per_s = best;
     return F2M_OK;
 }
 
@@ -1585,15 +1630,20 @@ f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int
     if (st != F2M_OK && st != kNeedsHost) {
         R->status = st;
         R->err = st == F2M_ERR_INPUT ? "invalid instance (fewer than 4 distinct points or degenerate box)"
-                                     : "instance exceeds a solver limit or did not converge";
+                 : st == F2M_ERR_CUDA ? "a grid barrier wait of the whole-GPU solver ran out "
+                                        "(grid_spin_limit polls); the solve was abandoned"
+                                      : "instance exceeds a solver limit or did not converge";
+        ctx->err = R->err;
         *out = R.release();
         return (f2m_status)st;
     }
     if ((s = pull_instance(ctx, C, 0, R->H, true))) return s;
     clk.mark("pull");
     if ((s = pull_stats(ctx, C, 0, *R))) return s;
-    // regular combs only: the device's primal stands; otherwise the host comb
-    // stage (Ax=b, repair loop) as the reference runs it
+    // every comb regular, or the irregular ones solved by Ax=b on the device:
+    // the device's primal stands; otherwise (an Ax=b system that did not
+    // converge, so the repair loop runs) the host comb stage as the
+    // reference runs it
     if ((s = (st == F2M_OK ? complete_from_device(ctx, C, 0, *R) : complete_instance(ctx, C, 0, prm, *R))))
         return s;
     clk.mark("complete");
@@ -1817,11 +1867,22 @@ cudaError_t smooth_steps_graph(f2m_ctx* ctx, SmoothBatch& B, bool grad) {
     return cudaGraphLaunch(ctx->sgraph, ctx->stream);
 }
 
+// Edge outputs of f2m_smoothed_bound_bwd_edges (all null for the other entries).
+struct SmoothEdgesOut {
+    int64_t cap = 0;
+    int64_t* n_edges = nullptr;
+    int32_t* a = nullptr;
+    int32_t* b = nullptr;
+    float* c = nullptr;
+    double* dc = nullptr;
+};
+
 // Shared body of the smoothed-bound entry points: buffers from the context's
 // arena, host inputs copied in, graph + bound (+ adjoint) on the device.
 f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const float* x,
                        const float* y, int32_t top_k, const f2m_smooth_params* p,
-                       const double* dL, double* L, float* gx, float* gy) {
+                       const double* dL, double* L, float* gx, float* gy,
+                       const SmoothEdgesOut* eo = nullptr) {
     if (!ctx) return F2M_ERR_INPUT;
     if (n_inst < 1 || !offs || !x || !y || !L) return fail(ctx, F2M_ERR_INPUT, "missing inputs");
     if (top_k < 3 || top_k > 64) return fail(ctx, F2M_ERR_INPUT, "top_k must be in [3, 64]");
@@ -1919,6 +1980,37 @@ f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const 
     if (gx) F2M_CUDA(cudaMemcpyAsync(gx, B.gx, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     if (gy) F2M_CUDA(cudaMemcpyAsync(gy, B.gy, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (eo && grad) {
+        // edges once each (lower point first, in the lower endpoint's list
+        // order) with dL/dc_e = the sum of the edge's two slot shares
+        int64_t S_used = 0;
+        F2M_CUDA(cudaMemcpy(&S_used, B.row + n, sizeof(int64_t), cudaMemcpyDeviceToHost));
+        std::vector<int64_t> row(n + 1), mir(S_used);
+        std::vector<int32_t> nb(S_used);
+        std::vector<float> cc(S_used);
+        std::vector<double> gc(S_used);
+        F2M_CUDA(cudaMemcpy(row.data(), B.row, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(nb.data(), B.nbr, S_used * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(mir.data(), B.mirror, S_used * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(cc.data(), B.c, S_used * sizeof(float), cudaMemcpyDeviceToHost));
+        F2M_CUDA(cudaMemcpy(gc.data(), B.gc, S_used * sizeof(double), cudaMemcpyDeviceToHost));
+        int64_t m = 0;
+        for (int32_t b = 0; b < n_inst; ++b)
+            for (int64_t g = offs[b]; g < offs[b + 1]; ++g)
+                for (int64_t k = row[g]; k < row[g + 1]; ++k) {
+                    const int64_t j = offs[b] + nb[k];
+                    if (j <= g) continue;
+                    if (m < eo->cap) {
+                        if (eo->a) eo->a[m] = (int32_t)g;
+                        if (eo->b) eo->b[m] = (int32_t)j;
+                        if (eo->c) eo->c[m] = cc[k];
+                        if (eo->dc) eo->dc[m] = gc[k] + gc[mir[k]];
+                    }
+                    ++m;
+                }
+        *eo->n_edges = m;
+        if (m > eo->cap) return fail(ctx, F2M_ERR_CAPACITY, "edge arrays hold fewer than the graph's edges");
+    }
     return F2M_OK;
 }
 
@@ -1936,6 +2028,23 @@ f2m_status f2m_smoothed_bound_bwd(f2m_ctx* ctx, int32_t n_inst, const int64_t* o
                                   const double* dL, double* L, float* dL_dx, float* dL_dy) {
     if (!dL_dx || !dL_dy) return ctx ? fail(ctx, F2M_ERR_INPUT, "dL_dx and dL_dy are required") : F2M_ERR_INPUT;
     return smooth_call(ctx, n_inst, offs, x, y, top_k, p, dL, L, dL_dx, dL_dy);
+}
+
+f2m_status f2m_smoothed_bound_bwd_edges(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const float* x,
+                                        const float* y, int32_t top_k, const f2m_smooth_params* p,
+                                        const double* dL, double* L, float* dL_dx, float* dL_dy,
+                                        int64_t edge_cap, int64_t* n_edges, int32_t* edge_a,
+                                        int32_t* edge_b, float* cost, double* dL_dc) {
+    if (!dL_dx || !dL_dy || !n_edges || edge_cap < 0)
+        return ctx ? fail(ctx, F2M_ERR_INPUT, "dL_dx, dL_dy and n_edges are required") : F2M_ERR_INPUT;
+    SmoothEdgesOut eo;
+    eo.cap = edge_cap;
+    eo.n_edges = n_edges;
+    eo.a = edge_a;
+    eo.b = edge_b;
+    eo.c = cost;
+    eo.dc = dL_dc;
+    return smooth_call(ctx, n_inst, offs, x, y, top_k, p, dL, L, dL_dx, dL_dy, &eo);
 }
 
 }  // extern "C"
@@ -2267,12 +2376,16 @@ void f2m_result_stats(const f2m_result* r, f2m_stats* s) { *s = r->st; }
 // forbids foreign cudaMalloc/cudaFree, or a latency-critical loop where a
 // cudaMalloc (which may synchronize the device and has no latency bound) is
 // not acceptable.  For them this entry point takes its scratch from one
-// fixed array in device memory, reserved when the library is loaded, and
-// allocates nothing itself: no cudaMalloc/cudaFree, no pinned or pageable
-// host buffers, no library call that allocates.  It is limited to one
-// instance of at most kNoAllocMaxPoints points and kNoAllocMaxN neighbours,
-// and it runs only the device stages (instances whose combs need the host
-// Ax=b stage are reported, not completed).
+// fixed array in device memory and allocates nothing itself: no
+// cudaMalloc/cudaFree, no pinned or pageable host buffers, no library call
+// that allocates.  With CUDA's lazy module loading (the default) the array and
+// the solver's kernels are put on a device by the first call there, so
+// callers make one warm-up call during their own set-up, before their pool
+// takes the GPU and before any stream capture (CUDA_MODULE_LOADING=EAGER
+// moves this to library load).  It is limited to one instance of at most
+// kNoAllocMaxPoints points and kNoAllocMaxN neighbours, always runs the
+// per-instance team solver, and runs only the device stages (instances whose
+// combs need the host Ax=b stage are reported, not completed).
 namespace {
 
 constexpr int32_t kNoAllocMaxPoints = 2048;
@@ -2289,7 +2402,10 @@ void* g_noalloc_addr[kNoAllocMaxDevices] = {};
 std::mutex g_noalloc_mu;
 
 // Device address of the scratch array on the current device, looked up the
-// first time this device is used.
+// first time this device is used.  A device reset (cudaDeviceReset, or
+// anything else that re-creates the primary context) unmaps the array and
+// leaves the saved address stale: callers of this entry point do not reset
+// the device between calls.
 cudaError_t noalloc_scratch(void** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -2333,6 +2449,7 @@ extern "C" f2m_status f2m_solve_points_noalloc(const double* d_x, const double* 
     if (n < 4 || top_k < 3) return F2M_ERR_INPUT;
     if (n > kNoAllocMaxPoints || top_k > kNoAllocMaxN) return F2M_ERR_CAPACITY;
     if (params && params->cost_mode != F2M_COST_REF_EUCLID) return F2M_ERR_INPUT;
+    if (params && params->solver == 2) return F2M_ERR_INPUT;  // the whole-GPU solver needs its own buffers
     f2m_params prm;
     f2m_default_params(&prm);
     if (params) prm = *params;

@@ -59,6 +59,10 @@ typedef struct f2m_params {
     int32_t cost_mode;     /* f2m_cost_mode */
     int32_t solver;        /* 0 auto: a team per instance, the whole GPU above 10,000 points;
                               2: the whole-GPU solver for a single instance of any size */
+    int64_t grid_spin_limit; /* the whole-GPU solver's grid barrier is a bounded wait: after
+                              this many polls a CTA gives up, every CTA leaves the solve and
+                              the call fails with F2M_ERR_CUDA (default 2^26, seconds of
+                              waiting; the GPU context stays usable).  Not in the reference. */
 } f2m_params;
 
 typedef struct f2m_ctx f2m_ctx;
@@ -116,6 +120,10 @@ typedef struct f2m_work {
     int64_t slot_iters;    /* sum over Jacobi iterations of the active slots read */
     int64_t slots;         /* CSR slots built (2 x edges) */
     int64_t points;        /* points after de-duplication */
+    int64_t pad_iters;     /* sum over Jacobi iterations of the list entries the warps sweep,
+                              padding of the 32-node slices included */
+    int64_t lane_iters;    /* sum over Jacobi iterations of the lanes updating a node
+                              (32 per slice of 32 nodes) */
 } f2m_work;
 
 /* Device time (CUDA events on the context stream) of the phases of the last
@@ -124,6 +132,14 @@ typedef struct f2m_work {
  * reference counterpart (the reference prints gettimeofday phase times,
  * graph_cuda_define.hpp:29-34). */
 f2m_status f2m_phase_times(f2m_ctx* ctx, float* ms, f2m_work* work);
+
+/* Measured FP64 pipe rate of this context's GPU in FP64 lane operations per
+ * second (diagnostics; no reference counterpart).  The dual descent issues
+ * FP64 additions and compares, so this rate, not HBM bandwidth, is the
+ * roofline of its persistent solver.  kind 0: independent DADD chains;
+ * kind 1: DSETP compares (one DADD per eight).  Best of `repeats` timed
+ * launches (CUDA events) over every SM at full occupancy. */
+f2m_status f2m_fp64_rate(f2m_ctx* ctx, int32_t kind, int32_t repeats, double* lane_ops_per_s);
 
 /* ------------------------------------------------------------------ */
 /* Single instance with full results (the F2M.h graph API).             */
@@ -183,14 +199,22 @@ f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k,
  * entry point allocates nothing: its scratch is one fixed 8 MiB array in
  * device memory that every GPU loading the library holds until exit.
  * Limits: n <= 2048 points, top_k <= 24, reference cost mode; larger inputs
- * return F2M_ERR_CAPACITY.  d_x, d_y (n coordinates), d_lp and d_status (one
+ * return F2M_ERR_CAPACITY.  It always runs the per-instance team solver:
+ * params->solver == 2 (the whole-GPU solver) returns F2M_ERR_INPUT.  d_x, d_y (n coordinates), d_lp and d_status (one
  * value each) are device pointers; `stream` is a cudaStream_t (NULL = the
  * legacy default stream).  The call only enqueues work on that stream and
  * returns; the results are ready once the stream is synchronised.  It runs
  * the device stages only: an instance whose combs need the host Ax=b stage
  * gets status F2M_ERR_CAPACITY (solve it with f2m_solve_points).
  * The first call on a device looks up the array's device address there
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * (cudaGetSymbolAddress) and, under CUDA's default lazy module loading, is
+ * also the moment the array and the solver's kernels are loaded onto that
+ * device -- the one time this entry point causes device allocations.  Make
+ * one warm-up call on each device during your own set-up, before your pool
+ * takes the GPU and before any stream capture (or set
+ * CUDA_MODULE_LOADING=EAGER to load at library load).  A device reset
+ * (cudaDeviceReset) makes the saved address stale: do not reset the device
+ * between calls.
  * All calls share the one array and it keeps the previous call's contents
  * (the solver clears what must start at zero), so calls that overlap on the
  * GPU -- on different streams, or from different host threads -- race. */
@@ -264,6 +288,22 @@ f2m_status f2m_smoothed_bound_bwd(f2m_ctx* ctx, int32_t n_inst, const int64_t* o
                                   const float* x, const float* y, int32_t top_k,
                                   const f2m_smooth_params* p, const double* dL, double* L,
                                   float* dL_dx, float* dL_dy);
+/* Backward with the edge-cost gradient exported: as f2m_smoothed_bound_bwd,
+ * plus the graph's edges and dL/dc_e, the derivative of sum_b dL[b] * L[b]
+ * with respect to each edge cost (at a stationary u, dL[b] * sigmoid(z_e):
+ * the smoothed x_e, whose sums over each point's edges are 2).  Edges are
+ * listed once, the lower global point index first (edge_a < edge_b, indices
+ * into x/y), in the order of the lower endpoint's list; cost is c_e in FP32.
+ * *n_edges receives the edge count; arrays of n_total * top_k entries always
+ * suffice (each point adds at most top_k edges to the union), and a smaller
+ * edge_cap returns F2M_ERR_CAPACITY with the count set.  Any edge array may
+ * be NULL. */
+f2m_status f2m_smoothed_bound_bwd_edges(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs,
+                                        const float* x, const float* y, int32_t top_k,
+                                        const f2m_smooth_params* p, const double* dL, double* L,
+                                        float* dL_dx, float* dL_dy, int64_t edge_cap,
+                                        int64_t* n_edges, int32_t* edge_a, int32_t* edge_b,
+                                        float* cost, double* dL_dc);
 int32_t f2m_smooth_max_nodes(void);
 
 /* Size classes of the batched solver (no reference counterpart): an instance

@@ -4,7 +4,9 @@
 # The recipe follows the reference's own makefile (nvcc for graph_cuda.cu,
 # g++ -std=c++11 for the host stage, nvcc to link RUN.cpp); the only additions
 # are the Boost stand-in header (refshim/) and an explicit sm_100a target.
-REF ?= /root/reference
+# the reference checkout: $(F2M_REFERENCE), else a sibling directory named
+# "reference" next to this repository
+REF ?= $(if $(F2M_REFERENCE),$(F2M_REFERENCE),$(abspath ../../reference))
 OUT := _ref
 NVCC ?= /usr/local/cuda/bin/nvcc
 CXX := $(shell test -x /usr/bin/g++ && echo /usr/bin/g++ || echo g++)

@@ -7,7 +7,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
+# The reference checkout (its examples are read by a few CPU tests): $F2M_REFERENCE,
+# else a sibling directory named "reference" next to this repository.
+REFERENCE = os.environ.get("F2M_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 
 
 def pytest_configure(config):

@@ -2,7 +2,8 @@
 
 1. reference_reports.json: the known answers shipped with the reference
    (examples/vsli/*.F2M_report and report_dir.txt), read from a local copy of
-   the reference repository (argument 1, default /root/reference).
+   the reference repository (argument 1; default $F2M_REFERENCE, else a sibling
+   checkout named "reference" next to this repository).
 2. oracle_*.npz: outputs of the CPU oracle (oracle/) on small seeded
    synthetic instances; the oracle is pinned to (1) by tests/test_oracle.py.
 
@@ -73,7 +74,10 @@ def save_case(name, gen, N, id_order):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    here = os.path.dirname(os.path.abspath(__file__))
+    default = os.environ.get("F2M_REFERENCE") or os.path.join(
+        os.path.dirname(os.path.dirname(os.path.dirname(here))), "reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else default
     if os.path.isdir(ref):
         with open(os.path.join(HERE, "reference_reports.json"), "w") as f:
             json.dump(reports(ref), f, indent=1)

@@ -22,6 +22,10 @@ def _close(a, b, rtol=LP_RTOL):
     return abs(a - b) <= rtol * max(abs(a), abs(b))
 
 
+AXB_XTOL = 1e-6   # x of an Ax=b comb edge solved on the device (rows in another order)
+AXB_LP_RTOL = 1e-9
+
+
 def _check_against(r, ref_status, ref_lp, ref_max_rank, lab1, lab2, Do, F, xval):
     assert r.status == ref_status
     assert np.array_equal(r.lab1, lab1), "kNN edge list differs"
@@ -29,9 +33,15 @@ def _check_against(r, ref_status, ref_lp, ref_max_rank, lab1, lab2, Do, F, xval)
     assert np.array_equal(r.Do, Do)
     assert np.array_equal(r.F, F), "potentials differ from the oracle"
     if ref_status == 0:
-        assert _close(r.lp, ref_lp)
         assert r.max_rank == ref_max_rank
-        assert np.array_equal(r.x, xval)
+        # x is identical except on the B edges of irregular combs whose Ax=b the
+        # device solved: the solution is the same, its last bits may not be
+        # (the reference takes the rows in its hash map's order)
+        simple = np.isin(xval, (0.0, 0.5, 1.0))
+        assert np.array_equal(r.x[simple], xval[simple])
+        assert np.all(np.abs(r.x - xval) <= AXB_XTOL)
+        exact = np.array_equal(r.x, xval)
+        assert _close(r.lp, ref_lp, LP_RTOL if exact else AXB_LP_RTOL)
 
 
 @pytest.mark.parametrize("name", ["uniform200_n10", "config1_n20", "lattice150_s1_n8",
@@ -376,8 +386,11 @@ def test_resume_from_stored_potentials(ctx):
 def test_grid_block_depths_give_identical_potentials(tmp_path):
     """Halo blocks recompute the nodes within k EF hops of each CTA's own
     nodes so that one grid barrier covers k Jacobi steps: the potentials must
-    not depend on k (0 = one grid barrier per step).  The depth is read once
-    per process, so each depth runs in a child process."""
+    not depend on k (0 = one grid barrier per step).  Depth 0 also launches
+    without halo storage (no shared scratch), so its partitions take the
+    thread-per-node global-memory path; depths 2 and 8 take the warp path in
+    shared memory.  The depth is read once per process, so each depth runs in
+    a child process."""
     import subprocess
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -413,3 +426,25 @@ def test_repeated_calls_are_bit_identical(ctx):
     r2 = ctx.solve_points(gx, gy, 16)
     assert np.array_equal(r1.F, r2.F) and np.array_equal(r1.x, r2.x)
     assert r1.lp == r2.lp and r1.stats == r2.stats
+
+
+def test_grid_barrier_wait_runs_out_and_the_context_recovers(ctx):
+    """The whole-GPU solver's grid barrier is a bounded wait.  With a limit of
+    one poll the first CTA to arrive gives up (nothing releases the barrier
+    that early), raises the error flag, every CTA leaves the solve and the
+    call fails with F2M_ERR_CUDA -- no fault, no trap.  The same context then
+    solves the instance normally, bit for bit as a fresh context does."""
+    import f2m_b200
+    x, y = synth.config2(7, n=12000)
+    short = f2m_b200.default_params(solver=2, grid_spin_limit=1)
+    with pytest.raises(f2m_b200.F2MError) as e:
+        ctx.solve_points(x, y, 16, params=short)
+    assert e.value.status == f2m_b200.ERR_CUDA
+    assert "barrier" in ctx.last_error()
+    r = ctx.solve_points(x, y, 16, params=f2m_b200.default_params(solver=2))
+    fresh = f2m_b200.Context(0)
+    try:
+        r2 = fresh.solve_points(x, y, 16, params=f2m_b200.default_params(solver=2))
+    finally:
+        fresh.close()
+    assert r.status == 0 and np.array_equal(r.F, r2.F) and r.lp == r2.lp

@@ -85,3 +85,30 @@ def test_cuda_path_matches_reference_program(ctx, name, tmp_path):
     assert _sha(base + ".F2M_solution") == str(g[name + "/sha_solution"])
     assert _sha(base + ".DM") == str(g[name + "/sha_dm"])
     assert _sha(path + "_duplicates") == str(g[name + "/sha_duplicates"])
+
+
+CLI = os.path.join(os.path.dirname(HERE), "f2m_b200", "bin", "F2M.solver.exe")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", _cases()[:4])
+def test_cli_binary_matches_reference_program(name, tmp_path):
+    """The drop-in binary itself (`F2M.solver.exe file N`, RUN.cpp:12-31) run
+    as a subprocess: the files it writes next to the input are byte-identical
+    to the reference program's and its report lines equal the reference's."""
+    import subprocess
+    assert os.path.exists(CLI), "F2M.solver.exe is not built (f2m_b200/build.py)"
+    g = _fixture()
+    N = MR.CASES[name][2]
+    path = MR.write_input(name, str(tmp_path))
+    r = subprocess.run([CLI, path, str(N)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Optimal Found: Yes" in r.stdout
+    base = f"{path}.top{N}"
+    lp_text, rank = _report(base + ".F2M_report")
+    assert lp_text == str(g[name + "/lp_text"])
+    assert rank == int(g[name + "/max_rank"])
+    assert f"Optimal Value: {lp_text}" in r.stdout
+    assert _sha(base + ".F2M_solution") == str(g[name + "/sha_solution"])
+    assert _sha(base + ".DM") == str(g[name + "/sha_dm"])
+    assert _sha(path + "_duplicates") == str(g[name + "/sha_duplicates"])
