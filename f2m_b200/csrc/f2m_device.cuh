@@ -313,4 +313,86 @@ static __device__ __noinline__ int axb_solve(const AxbRows& S, double* Aj, doubl
     return 0;
 }
 
+// Doubles of scratch one comb needs: its member list (m ints) and its system.
+__device__ __forceinline__ long long axb_comb_doubles(long long m, long long z) {
+    return (m + 1) / 2 + 1 + axb_scratch_doubles(m, z);
+}
+
+// B edges (|d| < porog) of node u over its whole list.
+template <class HP>
+__device__ __forceinline__ int count_b(const Slot* slot, const int64_t* row, HP H, int u, double porog) {
+    const double hu = H[u];
+    int z = 0;
+    for (int64_t a = row[u]; a < row[u + 1]; ++a) {
+        const double d = red_d(slot[a], u, H, hu);
+        if (d < porog && d > -porog) z++;
+    }
+    return z;
+}
+
+// One irregular comb's Ax=b, built and solved by one thread (out of line to
+// keep the solvers' registers free).  mem[0..m) are the comb's nodes in
+// ascending id (the rows); z their B edges (count_b summed); the system goes
+// to w (axb_scratch_doubles(m, z) doubles).  HP reads the potentials H = F/2,
+// LP the comb labels (the root of each node's comb, INT_MAX outside combs).
+// Writes x (FP32) of the comb's B edges whose larger-root comb is this one
+// (r) to both slots of the edge.  Returns 1 when the system did not converge
+// within 900 steps or a slot has no twin.
+template <class HP, class LP>
+__device__ __noinline__ int axb_comb(const Slot* slot, const int64_t* row, int64_t row0, const int32_t* mirror,
+                                     HP H, LP lab, const int* mem, int m, int z, int r, double porog, double* w,
+                                     float* xval) {
+    int* rs = reinterpret_cast<int*>(w);
+    int* col = rs + m + 1;
+    int* rhs = col + z;
+    int* vs = rhs + m;  // canonical slot (offset in the instance) of each variable
+    double* Aj = w + (2 * m + 2 * z + 2) / 2;
+    double* dd = Aj + m;
+    double* bg = dd + m;
+    double* x = bg + m;
+    double* xg = x + z;
+    int k = 0, q = 0;
+    for (int j = 0; j < m; ++j) {
+        const int u = mem[j];
+        const double hu = H[u];
+        int na = 0;
+        rs[j] = k;
+        for (int64_t a = row[u]; a < row[u + 1]; ++a) {
+            const Slot s = slot[a];
+            const double d = red_d(s, u, H, hu);
+            if (!(d < porog)) continue;
+            if (!(d > -porog)) { na++; continue; }
+            const int mi = mirror[a];
+            if (mi < 0 || k >= z) return 1;
+            const int cs = (int)((s.nbr > u ? a : row[s.nbr] + mi) - row0);
+            int t = 0;
+            while (t < q && vs[t] != cs) ++t;
+            if (t == q) vs[q++] = cs;
+            col[k++] = t;
+        }
+        rhs[j] = 2 - na;
+    }
+    rs[m] = k;
+    const AxbRows S{m, k, q, rs, col, rhs};
+    const int go = axb_solve(S, Aj, dd, bg, x, xg);
+    if (go == 0 || go > 900) return 1;
+    k = 0;
+    for (int j = 0; j < m; ++j) {
+        const int u = mem[j];
+        const double hu = H[u];
+        for (int64_t a = row[u]; a < row[u + 1]; ++a) {
+            const Slot s = slot[a];
+            const double d = red_d(s, u, H, hu);
+            if (!(d < porog) || !(d > -porog)) continue;
+            const int t = col[k++];
+            const int ln = lab[s.nbr];
+            if (ln != INT_MAX && ln > r) continue;  // the neighbour's comb decides
+            const float xv = (float)x[t];
+            xval[a] = xv;
+            xval[row[s.nbr] + mirror[a]] = xv;
+        }
+    }
+    return 0;
+}
+
 }  // namespace f2m

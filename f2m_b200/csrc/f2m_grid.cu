@@ -807,6 +807,58 @@ struct GridSolver {
         }
         nc = gsum_ll(nc);
         ni = gsum_ll(ni);
+        // irregular combs: Ax=b on the device (comb::solve_AxB,
+        // comb_thread.cpp:272-304), a thread per comb -- the thread owning
+        // its root.  The members of irregular combs are listed first as
+        // (root, node) keys in the ownership-sort buffer (free by now); each
+        // root's thread picks its own from that short list, in ascending
+        // node order, and builds the system in the slice arena (unused by
+        // this solver), handed out by an atomic counter.  The first solve
+        // only: after a repair shift the host driver runs the comb stage
+        // itself.  The instance goes to the host stage when a system does not
+        // converge within 900 steps or the arena is full.
+        bool solved = (ni == 0);
+        if (ni > 0 && !accumulate && !dead) {
+            unsigned long long* used = G.axb_used;      // [0] arena doubles, [1] listed members
+            for (int i = threadIdx.x; i < nown(); i += kGT) {
+                const int v = node(i);
+                const int l = vlab[v];
+                if (l == INT_MAX || !virr[l]) continue;
+                const unsigned long long k = atomicAdd(used + 1, 1ull);
+                G.okey[k] = ((unsigned long long)(unsigned)l << 32) | (unsigned)v;
+            }
+            sync();
+            const long long nm = (long long)*(volatile unsigned long long*)(used + 1);
+            long long bad = 0;
+            for (int i = threadIdx.x; i < nown() && !dead; i += kGT) {
+                const int r = node(i);
+                if (vlab[r] != r || !virr[r]) continue;
+                int m = 0, z = 0;
+                for (long long k = 0; k < nm; ++k) {
+                    const unsigned long long key = __ldcg(G.okey + k);
+                    if ((int)(key >> 32) != r) continue;
+                    m++;
+                    z += count_b(I.slot, I.row, hc(), (int)(unsigned)key, porog);
+                }
+                const unsigned long long need = (unsigned long long)axb_comb_doubles(m, z);
+                const unsigned long long off = atomicAdd(used, need);
+                if (off + need > (unsigned long long)B.S_cap) { bad = 1; continue; }
+                double* w = B.selD + off;
+                int* mem = reinterpret_cast<int*>(w);
+                int c = 0;
+                for (long long k = 0; k < nm && c < m; ++k) {  // members, insertion-sorted
+                    const unsigned long long key = __ldcg(G.okey + k);
+                    if ((int)(key >> 32) != r) continue;
+                    const int u = (int)(unsigned)key;
+                    int p = c++;
+                    while (p > 0 && mem[p - 1] > u) { mem[p] = mem[p - 1]; --p; }
+                    mem[p] = u;
+                }
+                bad |= axb_comb(I.slot, I.row, row0, B.mirror, hc(), vlab, mem, m, z, r, porog,
+                                w + (m + 1) / 2 + 1, B.xval);
+            }
+            solved = gsum_ll(bad) == 0;
+        }
         double lp = 0.0, dual_neg = 0.0, fsum = 0.0;
         long long maxr = -1, viol = 0;
         for (int i = threadIdx.x; i < nown(); i += kGT) {
@@ -819,14 +871,21 @@ struct GridSolver {
             for (int64_t a = r0; a < r1; ++a) {
                 const Slot s = I.slot[a];
                 const double d = red_d(s, v, hc(), hv);
-                const double x = (d < porog) ? ((d > -porog) ? 0.5 : 1.0) : 0.0;
-                B.xcode[a] = (uint8_t)(x == 1.0 ? 2 : (x == 0.5 ? 1 : 0));
+                double x = (d < porog) ? ((d > -porog) ? 0.5 : 1.0) : 0.0;
+                uint8_t code = (uint8_t)(x == 1.0 ? 2 : (x == 0.5 ? 1 : 0));
+                if (ni > 0 && solved && code == 1) {  // the edge's larger-root comb decides
+                    const int l1 = vlab[v], l2 = vlab[s.nbr];
+                    const int c = (l2 == INT_MAX) ? l1 : (l1 == INT_MAX ? l2 : ::max(l1, l2));
+                    if (c != INT_MAX && virr[c]) { x = (double)__ldcg(B.xval + a); code = 3; }
+                }
+                B.xcode[a] = code;
+                const bool in_x = (x != 0.0) || code == 3;  // every comb edge enters graph::X
                 degsum += (float)x;
-                any |= (x != 0.0);
+                any |= in_x;
                 if (s.nbr > v) {
                     lp += x * B.s_cost[a];
                     dual_neg += fmin(0.0, d);
-                    if (x != 0.0) maxr = ::max(maxr, (long long)::min((int)(a - r0), B.mirror[a]));
+                    if (in_x) maxr = ::max(maxr, (long long)::min((int)(a - r0), B.mirror[a]));
                 }
             }
             if (any && !(degsum > 2.0f - 1e-2f && degsum < 2.0f + 1e-2f)) viol++;
@@ -853,7 +912,7 @@ struct GridSolver {
             B.dual[b] = dmin * (-fsum + dual_neg);
             if (dead) { B.status[b] = F2M_ERR_CUDA; B.lp[b] = NAN; }
             else if (capped) { B.status[b] = F2M_ERR_NOT_CONVERGED; B.lp[b] = NAN; }
-            else if (ni > 0) { B.status[b] = kNeedsHost; B.lp[b] = NAN; }
+            else if (!solved) { B.status[b] = kNeedsHost; B.lp[b] = NAN; }
             else { B.status[b] = F2M_OK; B.lp[b] = lp; }
         }
     }
@@ -996,6 +1055,7 @@ cudaError_t launch_solve_grid(const Batch& B, const DevParams& P, const GridStat
     if (grid > kGridMaxCtas) grid = kGridMaxCtas;
     smem = grid_smem_bytes(V, grid, &cap, &nl, &ne);
     if ((e = cudaMemsetAsync(G.bar, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(G.axb_used, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(G.err, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
     Batch Bc = B;
     DevParams Pc = P;

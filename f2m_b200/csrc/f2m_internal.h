@@ -136,6 +136,7 @@ struct GridState {
     int32_t* irr;           // [V]
     unsigned* bar;          // [2] grid barrier: arrivals, generation
     int32_t* err;           // [1] set when a barrier timed out
+    unsigned long long* axb_used;  // [2] slice-arena doubles handed to Ax=b systems, comb members listed
     double* part;           // [2*grid] partial reductions
     long long* partl;       // [2*grid]
     int32_t* own;           // [V] nodes in ownership order (CTA c owns a contiguous run)

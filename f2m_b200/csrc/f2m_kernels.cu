@@ -872,81 +872,6 @@ __device__ __forceinline__ double half_grad(int n, Get get) {
     return (-(v1 + v2) / 2) * 0.5;
 }
 
-// One irregular comb's Ax=b, built and solved by one thread (the body of
-// Solver::axb_irregular, out of line to keep the solver's registers free).
-// The rows are the comb's nodes (lab[u] == r) in ascending id; the system
-// goes to the scratch at *w, which advances past it.  Writes x (FP32) of
-// the comb's B edges whose larger-root comb is this one to both slots of
-// the edge.  Returns 1 when the system did not converge within 900 steps
-// or a slot has no twin.
-__device__ __noinline__ int axb_comb(const Slot* slot, const int64_t* row, int64_t row0, const int32_t* mirror,
-                                     const double* H, const int* lab, int V, int r, double porog,
-                                     double** wp, float* xval) {
-    int m = 0, z = 0;
-    for (int u = 0; u < V; ++u) {
-        if (lab[u] != r) continue;
-        m++;
-        const double hu = H[u];
-        for (int64_t a = row[u]; a < row[u + 1]; ++a) {
-            const double d = red_d(slot[a], u, H, hu);
-            if (d < porog && d > -porog) z++;
-        }
-    }
-    double* w = *wp;
-    *wp = w + axb_scratch_doubles(m, z);
-    int* rs = reinterpret_cast<int*>(w);
-    int* col = rs + m + 1;
-    int* rhs = col + z;
-    int* vs = rhs + m;  // canonical slot (offset in the instance) of each variable
-    double* Aj = w + (2 * m + 2 * z + 2) / 2;
-    double* dd = Aj + m;
-    double* bg = dd + m;
-    double* x = bg + m;
-    double* xg = x + z;
-    int j = 0, k = 0, q = 0;
-    for (int u = 0; u < V; ++u) {
-        if (lab[u] != r) continue;
-        const double hu = H[u];
-        int na = 0;
-        rs[j] = k;
-        for (int64_t a = row[u]; a < row[u + 1]; ++a) {
-            const Slot s = slot[a];
-            const double d = red_d(s, u, H, hu);
-            if (!(d < porog)) continue;
-            if (!(d > -porog)) { na++; continue; }
-            const int mi = mirror[a];
-            if (mi < 0) return 1;
-            const int cs = (int)((s.nbr > u ? a : row[s.nbr] + mi) - row0);
-            int t = 0;
-            while (t < q && vs[t] != cs) ++t;
-            if (t == q) vs[q++] = cs;
-            col[k++] = t;
-        }
-        rhs[j++] = 2 - na;
-    }
-    rs[m] = k;
-    const AxbRows S{m, z, q, rs, col, rhs};
-    const int go = axb_solve(S, Aj, dd, bg, x, xg);
-    if (go == 0 || go > 900) return 1;
-    k = 0;
-    for (int u = 0; u < V; ++u) {
-        if (lab[u] != r) continue;
-        const double hu = H[u];
-        for (int64_t a = row[u]; a < row[u + 1]; ++a) {
-            const Slot s = slot[a];
-            const double d = red_d(s, u, H, hu);
-            if (!(d < porog) || !(d > -porog)) continue;
-            const int t = col[k++];
-            const int ln = lab[s.nbr];
-            if (ln != INT_MAX && ln > r) continue;  // the neighbour's comb decides
-            const float xv = (float)x[t];
-            xval[a] = xv;
-            xval[row[s.nbr] + mirror[a]] = xv;
-        }
-    }
-    return 0;
-}
-
 template <int TEAM>
 struct Solver {
     static constexpr int WARPS = TEAM / 32;
@@ -1178,19 +1103,6 @@ struct Solver {
         }
         return M_;
     }
-    // B edges (|d| < porog) of node u over its whole list; *nA = its A edges
-    // (d <= -porog), the host's classification (node::get_statusAB,
-    // node.cpp:49-57)
-    __device__ int count_ab(int u, double porog, int* nA) const {
-        const double hu = Hc[u];
-        int nb = 0, na = 0;
-        for (int64_t a = I.row[u]; a < I.row[u + 1]; ++a) {
-            const double d = red_d(I.slot[a], u, Hc, hu);
-            if (d < porog) { if (d > -porog) nb++; else na++; }
-        }
-        *nA = na;
-        return nb;
-    }
     // comb::solve_AxB (comb_thread.cpp:272-304) for every irregular comb of
     // the instance, on the device: a thread per comb (roots r = tid, tid +
     // TEAM, ...), its system in the instance's part of the global slice arena
@@ -1210,13 +1122,9 @@ struct Solver {
         for (int r = T.tid; r < V; r += TEAM) {
             if (lab[r] != r || !irr[r]) continue;
             long long m = 0, z = 0;
-            for (int u = 0; u < V; ++u) {
-                if (lab[u] != r) continue;
-                int na;
-                m++;
-                z += count_ab(u, porog, &na);
-            }
-            need += axb_scratch_doubles(m, z);
+            for (int u = 0; u < V; ++u)
+                if (lab[u] == r) { m++; z += count_b(I.slot, I.row, Hc, u, porog); }
+            need += axb_comb_doubles(m, z);
         }
         int total = 0;  // (a thread's share is clamped so that the team sum fits an int)
         const int off = T.excl_scan((int)::min(need, (long long)1 << 20), &total);
@@ -1225,7 +1133,13 @@ struct Solver {
         double* w = M.gsD + off;
         for (int r = T.tid; r < V && !bad; r += TEAM) {
             if (lab[r] != r || !irr[r]) continue;
-            bad = axb_comb(I.slot, I.row, row0, B.mirror, Hc, lab, V, r, porog, &w, B.xval);
+            int* mem = reinterpret_cast<int*>(w);
+            int m = 0, z = 0;
+            for (int u = 0; u < V; ++u)
+                if (lab[u] == r) { mem[m++] = u; z += count_b(I.slot, I.row, Hc, u, porog); }
+            double* sys = w + (m + 1) / 2 + 1;
+            w += axb_comb_doubles(m, z);
+            bad = axb_comb(I.slot, I.row, row0, B.mirror, Hc, lab, mem, m, z, r, porog, sys, B.xval);
         }
         return T.sum_ll(bad) == 0;
     }

@@ -209,6 +209,7 @@ void carve_grid(Arena& A, GridState& G, int64_t n, int64_t S) {
     G.irr = A.take<int32_t>(n);
     G.bar = A.take<unsigned>(4);
     G.err = A.take<int32_t>(4);
+    G.axb_used = A.take<unsigned long long>(2);
     G.part = A.take<double>(2 * kGridMaxCtas);
     G.partl = A.take<long long>(2 * kGridMaxCtas);
     G.own = A.take<int32_t>(n);
