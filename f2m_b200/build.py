@@ -9,7 +9,8 @@ LIB = os.path.join(HERE, "libf2m_b200.so")
 CLI = os.path.join(HERE, "bin", "F2M.solver.exe")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
-SOURCES = ["f2m_kernels.cu", "f2m_grid.cu", "f2m_smooth.cu", "f2m_probe.cu", "f2m_runtime.cu"]
+SOURCES = ["f2m_kernels.cu", "f2m_grid.cu", "f2m_smooth.cu", "f2m_probe.cu", "f2m_sort.cu",
+           "f2m_runtime.cu"]
 
 
 def _nvcc():

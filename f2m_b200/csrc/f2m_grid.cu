@@ -23,7 +23,6 @@
 #include <math.h>
 #include <stdint.h>
 
-#include <cub/device/device_radix_sort.cuh>
 
 #include "f2m_device.cuh"
 #include "f2m_internal.h"
@@ -1105,12 +1104,7 @@ __global__ void k_own_take(const unsigned long long* key, int n, int32_t* own) {
     if (i < n) own[i] = (int32_t)(unsigned)key[i];
 }
 
-size_t grid_order_temp_bytes(int64_t n) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, bytes, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                   (int)n, 32, 64);
-    return bytes;
-}
+size_t grid_order_temp_bytes(int64_t n) { return radix_sort_temp_bytes(n); }
 
 cudaError_t launch_grid_order(const Batch& B, const GridState& G, int b, int V, const int32_t* point_of,
                               bool spatial, cudaStream_t s, int64_t* launches) {
@@ -1118,14 +1112,13 @@ cudaError_t launch_grid_order(const Batch& B, const GridState& G, int b, int V, 
     const int T = 256, nb = (V + T - 1) / T;
     k_own_keys<<<nb, T, 0, s>>>(B, b, V, point_of, spatial ? 1 : 0, G.okey);
     ++*launches;
-    const unsigned long long* sorted = G.okey;
+    unsigned long long* sorted = G.okey;
     if (spatial) {
-        // the sort is stable, so equal codes keep the node order
-        size_t bytes = G.otmp_bytes;
-        cudaError_t e = cub::DeviceRadixSort::SortKeys(G.otmp, bytes, G.okey, G.okey2, V, 32, 64, s);
+        // by the code (bits 32-63); the sort is stable, so equal codes keep
+        // the node order
+        cudaError_t e = radix_sort(G.okey, G.okey2, nullptr, nullptr, V, 32, 64, G.otmp, G.otmp_bytes, s,
+                                   launches, &sorted, nullptr);
         if (e != cudaSuccess) return e;
-        ++*launches;
-        sorted = G.okey2;
     }
     k_own_take<<<nb, T, 0, s>>>(sorted, V, G.own);
     ++*launches;
@@ -1157,12 +1150,7 @@ __global__ void k_edge_cost_keys(Batch B, int b, int64_t S, const unsigned long 
     k2[i] = k1[i] == ~0ull ? ~0ull : (unsigned long long)__double_as_longlong(B.s_cost[s0 + v1[i]]);
 }
 
-size_t edge_order_temp_bytes(int64_t S) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                    (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)S);
-    return bytes;
-}
+size_t edge_order_temp_bytes(int64_t S) { return radix_sort_temp_bytes(S); }
 
 cudaError_t launch_edge_order(const Batch& B, int b, int V, int64_t S, const EdgeSort& E, const uint32_t** order,
                               cudaStream_t s, int64_t* launches) {
@@ -1171,17 +1159,17 @@ cudaError_t launch_edge_order(const Batch& B, int b, int V, int64_t S, const Edg
     k_edge_keys<<<(V + T - 1) / T, T, 0, s>>>(B, b, V, E.k1, E.v1);
     ++*launches;
     // LSD: by (emitter, partner), then stably by cost
-    size_t bytes = E.tmp_bytes;
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(E.tmp, bytes, E.k1, E.k2, E.v1, E.v2, (int)S, 0, 64, s);
+    unsigned long long* ks = nullptr;
+    uint32_t* vs = nullptr;
+    cudaError_t e = radix_sort(E.k1, E.k2, E.v1, E.v2, S, 0, 64, E.tmp, E.tmp_bytes, s, launches, &ks, &vs);
     if (e != cudaSuccess) return e;
+    unsigned long long* kc = (ks == E.k1) ? E.k2 : E.k1;  // the free key buffer
+    uint32_t* vfree = (vs == E.v1) ? E.v2 : E.v1;
+    k_edge_cost_keys<<<(unsigned)((S + T - 1) / T), T, 0, s>>>(B, b, S, ks, vs, kc);
     ++*launches;
-    k_edge_cost_keys<<<(unsigned)((S + T - 1) / T), T, 0, s>>>(B, b, S, E.k2, E.v2, E.k1);
-    ++*launches;
-    bytes = E.tmp_bytes;
-    e = cub::DeviceRadixSort::SortPairs(E.tmp, bytes, E.k1, E.k2, E.v2, E.v1, (int)S, 0, 64, s);
+    e = radix_sort(kc, ks, vs, vfree, S, 0, 64, E.tmp, E.tmp_bytes, s, launches, &ks, &vs);
     if (e != cudaSuccess) return e;
-    ++*launches;
-    *order = E.v1;
+    *order = vs;
     return cudaGetLastError();
 }
 

@@ -239,6 +239,12 @@ int32_t smooth_max_nodes();
 
 cudaError_t launch_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* scratch,
                         cudaStream_t s, int64_t* launches);
+// Stable LSD radix sort of 64-bit keys (values optional) by bits [begin_bit,
+// end_bit) (f2m_sort.cu); the result ends in keys/vals or kbuf/vbuf (*kres, *vres).
+size_t radix_sort_temp_bytes(int64_t n);
+cudaError_t radix_sort(unsigned long long* keys, unsigned long long* kbuf, uint32_t* vals, uint32_t* vbuf,
+                       int64_t n, int begin_bit, int end_bit, void* temp, size_t temp_bytes, cudaStream_t s,
+                       int64_t* launches, unsigned long long** kres, uint32_t** vres);
 int64_t scan_scratch_elems(int64_t n);
 int32_t solve_max_nodes();
 
