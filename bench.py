@@ -48,13 +48,13 @@ LP_TOL = 1e-9
 # its source (f2m_kernels.cu Solver::step / slice_hgrad / half_grad,
 # f2m_device.cuh top3_insert):
 #   per list entry a warp lane sweeps (padding of the 32-node slices
-#   included): 2 DADD for the reduced cost (D + H[lo]) + H[hi] and 2 DSETP
+#   included): 2 DADD for the reduced cost (D + H[lo]) + H[hi] and 3 DSETP
 #   for the top-3 insertion;
 #   per lane updating a node: 1 DSETP (first value below the 1e6 sentinels),
 #   1 DADD (v1 + v2), 2 DMUL (/2, *0.5) and 1 DADD (H + grad/2).
 # Partitions, gradient checks and comb extraction are not counted, so the
 # fraction is a lower bound.
-FP64_PER_ENTRY = 4
+FP64_PER_ENTRY = 5
 FP64_PER_LANE = 5
 
 

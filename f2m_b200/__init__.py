@@ -73,7 +73,7 @@ class BatchOut(ctypes.Structure):
     _fields_ = [("lp", ctypes.c_void_p), ("status", ctypes.c_void_p),
                 ("n_nodes", ctypes.c_void_p), ("n_edges", ctypes.c_void_p),
                 ("n_combs", ctypes.c_void_p), ("max_rank", ctypes.c_void_p),
-                ("iterations", ctypes.c_void_p)]
+                ("iterations", ctypes.c_void_p), ("n_irregular", ctypes.c_void_p)]
 
 
 class SmoothParams(ctypes.Structure):
@@ -246,7 +246,8 @@ class Context:
         extra = {}
         if details:
             for k, dt in (("n_nodes", np.int32), ("n_edges", np.int32), ("n_combs", np.int32),
-                          ("max_rank", np.int32), ("iterations", np.int64)):
+                          ("max_rank", np.int32), ("iterations", np.int64),
+                          ("n_irregular", np.int32)):
                 extra[k] = np.zeros(n, dt)
                 setattr(o, k, extra[k].ctypes.data)
         p = params if params is not None else default_params()

@@ -124,7 +124,8 @@ struct Inst {
     int64_t base;          // first node index
     const int64_t* row;    // row[v], v in [0, V]
     const Slot* slot;
-    uint16_t* perm;
+    uint16_t* perm;        // per-node list order (the reference's permuted pointer list)
+    Slot* pslot;           // the slots in that order, so a scan reads one record per position
     double* gD;            // global EF arena of this instance (D)
     uint16_t* gN;          // (neighbour)
 };
@@ -137,6 +138,7 @@ __device__ __forceinline__ Inst make_inst(const Batch& B, int b) {
     I.row = B.row + I.base;
     I.slot = B.slot;
     I.perm = B.perm;
+    I.pslot = B.pslot;
     I.gD = B.efD + I.row[0];
     I.gN = B.efN + I.row[0];
     return I;
@@ -152,41 +154,30 @@ __device__ __forceinline__ double red_d(const Slot& s, int v, HP H, double hv) {
 
 // Sorted insertion of x into (v0 <= v1 <= v2) keeping the three smallest:
 // the reference's compare chain (strict <, so ties and NaN leave the triple
-// as it is) written as two FP64 compares and integer selects.  x < v1 decides
-// the half: if it holds, x < v2 holds too and only x < v0 is open; if not,
-// x < v0 fails too and only x < v2 is open.  One select picks the bound of
-// the open compare.  The selects run on the integer pipe; the FP64 pipe,
-// which bounds the dual step on this GPU, sees two compares per entry.
+// as it is) written as three independent FP64 compares and integer selects.
+// The step is bound by latency, not by the FP64 pipe (measured: about a
+// tenth of its rate), and the insertion is the loop-carried chain of a
+// lane: three compares issued together keep it at one compare and two
+// selects deep (a two-compare form, x < v1 first, then x against v0 or v2,
+// is one compare deeper and measured slower).
 __device__ __forceinline__ void top3_insert(double x, double& v0, double& v1, double& v2) {
-    const bool c1 = x < v1;
-    const bool cy = x < (c1 ? v0 : v2);
-    const bool c0 = c1 && cy, c2 = c1 || cy;
+    const bool c0 = x < v0, c1 = x < v1, c2 = x < v2;
     v2 = c1 ? v1 : (c2 ? x : v2);
     v1 = c0 ? v0 : (c1 ? x : v1);
     v0 = c0 ? x : v0;
 }
+// Reduced cost of position k of node v's list (the slot perm[r0 + k]).
 template <class HP>
-__device__ __forceinline__ double pdv(const Inst& I, int64_t r0, const uint16_t* list, int k, int v, HP H,
-                                      double hv) {
-    return red_d(I.slot[r0 + list[k]], v, H, hv);
+__device__ __forceinline__ double pdv(const Inst& I, int64_t r0, int k, int v, HP H, double hv) {
+    return red_d(I.pslot[r0 + k], v, H, hv);
+}
+// Sets pslot from slot and perm for nodes [v0, V) in steps of `step` (each
+// solver keeps the two in step from there: every swap moves both).
+__device__ __forceinline__ void init_pslot(const Inst& I, int v0, int step) {
+    for (int v = v0; v < I.V; v += step)
+        for (int64_t a = I.row[v]; a < I.row[v + 1]; ++a) I.pslot[a] = I.slot[I.row[v] + I.perm[a]];
 }
 
-// qpart_ptr_B (graph_cuda_partition.hpp:3-25), the bound tested first.  On
-// finite values it performs at most size/2 swaps; the pass cap only matters
-// for NaN values (where the reference loops forever) and keeps the kernel
-// finite.
-template <class HP>
-static __device__ int qpart_b(const Inst& I, int64_t r0, int v, HP H, int size, double avg) {
-    uint16_t* list = I.perm + r0;
-    const double hv = H[v];
-    int low = 0, high = size - 1, i = low, j = high;
-    for (int pass = 0; i < j && pass <= size; ++pass) {
-        while (i <= high && pdv(I, r0, list, i, v, H, hv) <= avg) i++;
-        while (j >= low && pdv(I, r0, list, j, v, H, hv) > avg) j--;
-        if (i < j) { const uint16_t t = list[i]; list[i] = list[j]; list[j] = t; }
-    }
-    return j + 1;
-}
 // The threshold loop of qpart_ptr_EF, `while (avg < g && bump < limit) {
 // avg += 1; ++bump; }`, with the stretches where every `+= 1` is exact taken
 // in one addition: above 1 inside a binade (ulp <= 1 and no carry into the
@@ -219,32 +210,84 @@ __device__ __forceinline__ void bump_until(double& avg, int& bump, double g, int
     }
 }
 
-// qpart_ptr_EF (graph_cuda_partition.hpp:27-54): raise the threshold by 1
-// until at least ef_min entries qualify (bounded: see qpart_b).
+// qpart_ptr_B / qpart_ptr_EF (graph_cuda_partition.hpp:3-54) with the
+// scans' loads run ahead: every reduced cost is a chain of dependent loads
+// (the position's slot record from L2, then the neighbour's potential), so
+// the scans evaluate kPf positions at once and then test them in order, and
+// the loads of a chunk overlap.  Positions are read from pslot, the slots
+// kept in list order, and every swap moves both the list (perm, which the
+// host stage and the repair loop read) and pslot.  The tests (the bound first, as the reference's loop
+// reads one element past either end), the swaps and the threshold sequence
+// are the reference's, so the final order and count are too.  On finite
+// values a pass performs at most size/2 swaps; the pass cap only matters for
+// NaN values, where the reference loops forever.
 //
-// A pass whose threshold t stays below the smallest value g of the upper part
-// left by the previous pass finds the list already partitioned for t: the
-// i-scan stops at the first upper entry, the j-scan at the last lower one, no
-// swap happens and the count repeats.  Such passes are counted but not run,
-// so the threshold sequence (repeated FP64 `avg += 1`), the final order and
-// the count are those of the plain loop.  With a NaN in the list every pass
-// runs.
+// qpart_ef_la raises the threshold by 1 until at least ef_min entries
+// qualify.  A pass whose threshold t stays below the smallest value g of the
+// upper part left by the previous pass finds the list already partitioned
+// for t: the i-scan stops at the first upper entry, the j-scan at the last
+// lower one, no swap happens and the count repeats.  Such passes are counted
+// but not run (bump_until), so the threshold sequence (repeated FP64
+// `avg += 1`), the final order and the count are those of the plain loop.
+// With a NaN in the list every pass runs.
+constexpr int kPf = 8;
 template <class HP>
-static __device__ int qpart_ef(const Inst& I, int64_t r0, int v, HP H, int size, double avg,
-                               int ef_min) {
-    if (size < ef_min) return size;  // the reference would not terminate
+__device__ __forceinline__ int qpart_b_la(const Inst& I, int64_t r0, int v, HP H, int size, double avg) {
+    uint16_t* list = I.perm + r0;
+    const double hv = H[v];
+    int low = 0, high = size - 1, i = low, j = high;
+    for (int pass = 0; i < j && pass <= size; ++pass) {
+        for (bool go = true; go;) {  // while (i <= high && pdv(i) <= avg) i++
+            double d[kPf];
+#pragma unroll
+            for (int c = 0; c < kPf; ++c) d[c] = (i + c <= high) ? pdv(I, r0, i + c, v, H, hv) : 0.0;
+#pragma unroll
+            for (int c = 0; c < kPf; ++c)
+                if (go) {
+                    if (i <= high && d[c] <= avg) ++i;
+                    else go = false;
+                }
+        }
+        for (bool go = true; go;) {  // while (j >= low && pdv(j) > avg) j--
+            double d[kPf];
+#pragma unroll
+            for (int c = 0; c < kPf; ++c) d[c] = (j - c >= low) ? pdv(I, r0, j - c, v, H, hv) : 0.0;
+#pragma unroll
+            for (int c = 0; c < kPf; ++c)
+                if (go) {
+                    if (j >= low && d[c] > avg) --j;
+                    else go = false;
+                }
+        }
+        if (i < j) {
+            const uint16_t t = list[i]; list[i] = list[j]; list[j] = t;
+            Slot* ps = I.pslot + r0;
+            const Slot u = ps[i]; ps[i] = ps[j]; ps[j] = u;
+        }
+    }
+    return j + 1;
+}
+template <class HP>
+__device__ __forceinline__ int qpart_ef_la(const Inst& I, int64_t r0, int v, HP H, int size, double avg,
+                                           int ef_min) {
+    if (size < ef_min) return size;
     constexpr int kLimit = 1 << 20;
-    const uint16_t* list = I.perm + r0;
     const double hv = H[v];
     for (int bump = 0; bump < kLimit;) {
-        const int p = qpart_b(I, r0, v, H, size, avg);
+        const int p = qpart_b_la(I, r0, v, H, size, avg);
         if (p >= ef_min) return p;
         double g = INFINITY;
         bool nan = false;
-        for (int k = 0; k < size; ++k) {
-            const double d = pdv(I, r0, list, k, v, H, hv);
-            nan |= (d != d);
-            if (k >= p) g = fmin(g, d);
+        for (int k0 = 0; k0 < size; k0 += kPf) {
+            double d[kPf];
+#pragma unroll
+            for (int c = 0; c < kPf; ++c) d[c] = (k0 + c < size) ? pdv(I, r0, k0 + c, v, H, hv) : 0.0;
+#pragma unroll
+            for (int c = 0; c < kPf; ++c)
+                if (k0 + c < size) {
+                    nan |= (d[c] != d[c]);
+                    if (k0 + c >= p) g = fmin(g, d[c]);
+                }
         }
         avg += 1;
         ++bump;

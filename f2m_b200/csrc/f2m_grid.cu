@@ -108,74 +108,6 @@ __device__ __forceinline__ double grad_half(int n, const double* Dp, const uint3
     return (-(a1 + a2) / 2) * 0.5;
 }
 
-// qpart_ptr_B / qpart_ptr_EF (graph_cuda_partition.hpp:3-54) for the grid
-// solver, where every reduced cost is a chain of three global loads (list
-// position, slot, neighbour potential through L2).  The scans evaluate kPf
-// positions ahead and then test them in order, so the loads of a chunk
-// overlap; the tests, the swaps, the threshold sequence and therefore the
-// final order and count are those of qpart_b / qpart_ef.
-constexpr int kPf = 8;
-__device__ __forceinline__ int qpart_b_g(const Inst& I, int64_t r0, int v, L2Ptr H, int size, double avg) {
-    uint16_t* list = I.perm + r0;
-    const double hv = H[v];
-    int low = 0, high = size - 1, i = low, j = high;
-    for (int pass = 0; i < j && pass <= size; ++pass) {
-        for (bool go = true; go;) {  // while (i <= high && pdv(i) <= avg) i++
-            double d[kPf];
-#pragma unroll
-            for (int c = 0; c < kPf; ++c) d[c] = (i + c <= high) ? pdv(I, r0, list, i + c, v, H, hv) : 0.0;
-#pragma unroll
-            for (int c = 0; c < kPf; ++c)
-                if (go) {
-                    if (i <= high && d[c] <= avg) ++i;
-                    else go = false;
-                }
-        }
-        for (bool go = true; go;) {  // while (j >= low && pdv(j) > avg) j--
-            double d[kPf];
-#pragma unroll
-            for (int c = 0; c < kPf; ++c) d[c] = (j - c >= low) ? pdv(I, r0, list, j - c, v, H, hv) : 0.0;
-#pragma unroll
-            for (int c = 0; c < kPf; ++c)
-                if (go) {
-                    if (j >= low && d[c] > avg) --j;
-                    else go = false;
-                }
-        }
-        if (i < j) { const uint16_t t = list[i]; list[i] = list[j]; list[j] = t; }
-    }
-    return j + 1;
-}
-__device__ __forceinline__ int qpart_ef_g(const Inst& I, int64_t r0, int v, L2Ptr H, int size, double avg,
-                                          int ef_min) {
-    if (size < ef_min) return size;
-    constexpr int kLimit = 1 << 20;
-    const uint16_t* list = I.perm + r0;
-    const double hv = H[v];
-    for (int bump = 0; bump < kLimit;) {
-        const int p = qpart_b_g(I, r0, v, H, size, avg);
-        if (p >= ef_min) return p;
-        double g = INFINITY;
-        bool nan = false;
-        for (int k0 = 0; k0 < size; k0 += kPf) {
-            double d[kPf];
-#pragma unroll
-            for (int c = 0; c < kPf; ++c) d[c] = (k0 + c < size) ? pdv(I, r0, list, k0 + c, v, H, hv) : 0.0;
-#pragma unroll
-            for (int c = 0; c < kPf; ++c)
-                if (k0 + c < size) {
-                    nan |= (d[c] != d[c]);
-                    if (k0 + c >= p) g = fmin(g, d[c]);
-                }
-        }
-        avg += 1;
-        ++bump;
-        if (nan) continue;
-        bump_until(avg, bump, g, kLimit);
-    }
-    return size;
-}
-
 // qpart_ptr_EF on a node's list copied to shared memory: `pl` holds the list
 // order and `val` the reduced cost of each position.  The loop is qpart_ef's
 // (the Hoare scans, the swaps, which move both arrays, and the threshold
@@ -439,7 +371,7 @@ struct GridSolver {
             const int64_t go = r0 - row0;
             const bool sm = lo + n <= cap;
             for (int k = 0; k < n; ++k) {
-                const Slot s = I.slot[r0 + I.perm[r0 + k]];
+                const Slot s = I.pslot[r0 + k];
                 const uint32_t w = (uint32_t)s.nbr | (s.nbr < v ? 0x80000000u : 0u);
                 G.gD[go + k] = s.D;
                 G.gW[go + k] = w;
@@ -638,10 +570,10 @@ struct GridSolver {
                 double avg = thr;
                 if (glob) {
                     const double hv = H[v];
-                    avg = pdv(I, r0, I.perm + r0, 0, v, H, hv);
-                    for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, I.perm + r0, k, v, H, hv));
+                    avg = pdv(I, r0, 0, v, H, hv);
+                    for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, k, v, H, hv));
                 }
-                G.efc[v] = qpart_ef_g(I, r0, v, H, d, avg, P.ef_min);
+                G.efc[v] = qpart_ef_la(I, r0, v, H, d, avg, P.ef_min);
             }
             __syncthreads();
             return;
@@ -673,16 +605,19 @@ struct GridSolver {
                     p = qpart_ef_vals(pl, val, d, avg, P.ef_min);
                 }
                 __syncwarp();
-                for (int k = lane; k < d; k += 32) list[k] = pl[k];
+                for (int k = lane; k < d; k += 32) {
+                    list[k] = pl[k];
+                    I.pslot[r0 + k] = I.slot[r0 + pl[k]];
+                }
                 __syncwarp();
             } else if (lane == 0) {
                 double avg = thr;
                 if (glob) {
                     const double hv = H[v];
-                    avg = pdv(I, r0, list, 0, v, H, hv);
-                    for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, list, k, v, H, hv));
+                    avg = pdv(I, r0, 0, v, H, hv);
+                    for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, k, v, H, hv));
                 }
-                p = qpart_ef_g(I, r0, v, H, d, avg, P.ef_min);
+                p = qpart_ef_la(I, r0, v, H, d, avg, P.ef_min);
             }
             if (lane == 0) G.efc[v] = p;
         }
@@ -744,7 +679,7 @@ struct GridSolver {
         int* lab = G.scratch + V;
         for (int i = threadIdx.x; i < nown(); i += kGT) {  // cuda_partition_v3
             const int v = node(i);
-            ccnt[v] = qpart_b_g(I, I.row[v], v, hc(), G.efc[v], P.comb_thr);
+            ccnt[v] = qpart_b_la(I, I.row[v], v, hc(), G.efc[v], P.comb_thr);
         }
         for (int i = threadIdx.x; i < nown(); i += kGT) {
             const int v = node(i);
@@ -752,7 +687,7 @@ struct GridSolver {
             const double hv = hc()[v];
             bool has = false;
             for (int k = 0; k < ccnt[v] && !has; ++k) {
-                const double d = pdv(I, r0, I.perm + r0, k, v, hc(), hv);
+                const double d = pdv(I, r0, k, v, hc(), hv);
                 has = (d >= -porog && d <= porog);
             }
             lab[v] = has ? v : INT_MAX;
@@ -770,7 +705,7 @@ struct GridSolver {
                 const int64_t r0 = I.row[v];
                 const double hv = hc()[v];
                 for (int k = 0; k < ccnt[v]; ++k) {
-                    const Slot s = I.slot[r0 + I.perm[r0 + k]];
+                    const Slot s = I.pslot[r0 + k];
                     const double d = red_d(s, v, hc(), hv);
                     if (d >= -porog && d <= porog) m = min(m, vlab[s.nbr]);
                 }
@@ -961,6 +896,11 @@ __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, Gri
     S.L.ne = ne;
     S.L.kmax = min(kmax, kMaxBlk);
     double M;
+    // the own nodes' slots in list order (the host paths upload slot and perm)
+    for (int i = threadIdx.x; i < nv; i += kGT) {
+        const int v = S.node(i);
+        for (int64_t a = I.row[v]; a < I.row[v + 1]; ++a) I.pslot[a] = I.slot[I.row[v] + I.perm[a]];
+    }
     if (!refit) {
         for (int i = threadIdx.x; i < nv; i += kGT) {
             const int v = S.node(i);

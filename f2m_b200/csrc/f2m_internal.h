@@ -87,6 +87,7 @@ struct Batch {
     int32_t* s_oth;         // [S]
     Slot* slot;             // [S]
     uint16_t* perm;         // [S] per-node list order (local positions)
+    Slot* pslot;            // [S] the slots in list order: pslot[r+k] = slot[r + perm[r+k]]
     int32_t* mirror;        // [S] position of the same edge in the neighbour's list
     double* efD;            // [S] active-set arena (update_EF copies): D
     uint16_t* efN;          // [S] active-set arena: neighbour

@@ -548,6 +548,7 @@ __global__ void __launch_bounds__(kT) k_graph_sort(Batch B) {
         s.aux = (int32_t)(a - r0);
         B.slot[a] = s;
         B.perm[a] = (uint16_t)(a - r0);
+        B.pslot[a] = s;
     }
 }
 
@@ -959,7 +960,7 @@ struct Solver {
                 const int64_t go = r0 - row0;
                 const int n = M.cnt[v];
                 for (int k = 0; k < n; ++k) {
-                    const Slot s = I.slot[r0 + I.perm[r0 + k]];
+                    const Slot s = I.pslot[r0 + k];
                     I.gD[go + k] = s.D;
                     I.gN[go + k] = ef_word(v, s.nbr);
                 }
@@ -1040,7 +1041,7 @@ struct Solver {
     __device__ double check_opt() {
         for (int v = T.tid; v < I.V; v += TEAM) {
             const int d = deg(v);
-            M.cnt[v] = (d < P.ef_small_deg) ? d : qpart_ef(I, I.row[v], v, Hc, d, P.ef_thr, P.ef_min);
+            M.cnt[v] = (d < P.ef_small_deg) ? d : qpart_ef_la(I, I.row[v], v, Hc, d, P.ef_thr, P.ef_min);
         }
         finish_partition();
         checks++;
@@ -1070,9 +1071,9 @@ struct Solver {
                 if (d < P.glob_K) { M.cnt[v] = d; continue; }
                 const int64_t r0 = I.row[v];
                 const double hv = Hc[v];
-                double avg = pdv(I, r0, I.perm + r0, 0, v, Hc, hv);
-                for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, I.perm + r0, k, v, Hc, hv));
-                M.cnt[v] = qpart_ef(I, r0, v, Hc, d, avg, P.ef_min);
+                double avg = pdv(I, r0, 0, v, Hc, hv);
+                for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, k, v, Hc, hv));
+                M.cnt[v] = qpart_ef_la(I, r0, v, Hc, d, avg, P.ef_min);
             }
             finish_partition();
             if (grad_max() < P.glob_tol) break;
@@ -1151,14 +1152,14 @@ struct Solver {
         int* ccnt = reinterpret_cast<int*>(Hn);  // Hn is free: room for 2V ints
         int* lab = ccnt + V;
         for (int v = T.tid; v < V; v += TEAM)  // cuda_partition_v3
-            ccnt[v] = qpart_b(I, I.row[v], v, Hc, M.cnt[v], P.comb_thr);
+            ccnt[v] = qpart_b_la(I, I.row[v], v, Hc, M.cnt[v], P.comb_thr);
         T.sync();
         for (int v = T.tid; v < V; v += TEAM) {
             const int64_t r0 = I.row[v];
             const double hv = Hc[v];
             bool has = false;
             for (int k = 0; k < ccnt[v] && !has; ++k) {
-                const double d = pdv(I, r0, I.perm + r0, k, v, Hc, hv);
+                const double d = pdv(I, r0, k, v, Hc, hv);
                 has = (d >= -porog && d <= porog);
             }
             lab[v] = has ? v : INT_MAX;
@@ -1176,7 +1177,7 @@ struct Solver {
                 const int64_t r0 = I.row[v];
                 const double hv = Hc[v];
                 for (int k = 0; k < ccnt[v]; ++k) {
-                    const Slot s = I.slot[r0 + I.perm[r0 + k]];
+                    const Slot s = I.pslot[r0 + k];
                     const double d = red_d(s, v, Hc, hv);
                     if (d >= -porog && d <= porog) m = min(m, vlab[s.nbr]);
                 }
@@ -1305,6 +1306,7 @@ __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, con
             continue;
         }
         const TeamMem M = carve_team(mine, team_bytes, B, b, I.V);  // sized for this instance
+        init_pslot(I, T.tid, TEAM);  // the host paths upload slot and perm only
         Solver<TEAM> S(B, P, I, T, M);
         double Mg;
         if (!REFIT) {

@@ -272,6 +272,7 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.s_oth = A.take<int32_t>(S);
     B.slot = A.take<Slot>(S);
     B.perm = A.take<uint16_t>(S);
+    B.pslot = A.take<Slot>(S);
     B.mirror = A.take<int32_t>(S);
     B.efD = A.take<double>(S);
     B.efN = A.take<uint16_t>(S);
@@ -1489,6 +1490,7 @@ f2m_status f2m_solve_batch(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, co
     if (out->n_edges) F2M_CUDA(cudaMemcpyAsync(out->n_edges, C.B.n_edges, n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     if (out->n_combs) F2M_CUDA(cudaMemcpyAsync(out->n_combs, C.B.n_combs, n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     if (out->iterations) F2M_CUDA(cudaMemcpyAsync(out->iterations, C.B.iters, n_inst * sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    if (out->n_irregular) F2M_CUDA(cudaMemcpyAsync(out->n_irregular, C.B.n_irr, n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
     if ((s = complete_batch(ctx, C, prm, status, lp, out->max_rank ? &mr : nullptr))) return s;
     std::memcpy(out->status, status.data(), n_inst * sizeof(int32_t));
@@ -1538,6 +1540,7 @@ f2m_status f2m_solve_batch_device(f2m_ctx* ctx, int32_t n_inst, const int64_t* h
     F2M_CUDA(cp(d_out->n_combs, C.B.n_combs, n_inst * sizeof(int32_t)));
     F2M_CUDA(cp(d_out->max_rank, C.B.max_rank, n_inst * sizeof(int32_t)));
     F2M_CUDA(cp(d_out->iterations, C.B.iters, n_inst * sizeof(int64_t)));
+    F2M_CUDA(cp(d_out->n_irregular, C.B.n_irr, n_inst * sizeof(int32_t)));
     return F2M_OK;
 }
 
@@ -2391,7 +2394,7 @@ namespace {
 
 constexpr int32_t kNoAllocMaxPoints = 2048;
 constexpr int32_t kNoAllocMaxN = 24;
-constexpr size_t kNoAllocBytes = (size_t)8 << 20;  // 8 MiB of device memory per GPU
+constexpr size_t kNoAllocBytes = (size_t)12 << 20;  // 12 MiB of device memory per GPU
 
 // The scratch of f2m_solve_points_noalloc.  In host code this name is only a
 // stand-in for the device symbol: its device address comes from

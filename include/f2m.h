@@ -96,6 +96,8 @@ typedef struct f2m_batch_out {
     int32_t* n_combs;      /* optional [n_inst] */
     int32_t* max_rank;     /* optional [n_inst] "MAX edge rank" */
     int64_t* iterations;   /* optional [n_inst] Jacobi iterations */
+    int32_t* n_irregular;  /* optional [n_inst] combs failing 2A+B=4, whose x comes from Ax=b
+                              (comb_thread.cpp:272-304) */
 } f2m_batch_out;
 
 /* Host arrays: offs[n_inst+1] (int64) into x[], y[] (FP64 coordinates,
@@ -196,7 +198,7 @@ f2m_status f2m_solve_file(f2m_ctx* ctx, const char* path, int32_t top_k,
  * For callers that cannot allocate device memory while they run -- a host
  * application that owns the GPU through its own memory pool, or a
  * latency-bound loop that cannot afford cudaMalloc's synchronisation -- this
- * entry point allocates nothing: its scratch is one fixed 8 MiB array in
+ * entry point allocates nothing: its scratch is one fixed 12 MiB array in
  * device memory that every GPU loading the library holds until exit.
  * Limits: n <= 2048 points, top_k <= 24, reference cost mode; larger inputs
  * return F2M_ERR_CAPACITY.  It always runs the per-instance team solver:

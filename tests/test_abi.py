@@ -52,3 +52,17 @@ def test_cli_usage_without_arguments():
         pytest.skip("CLI not built")
     out = subprocess.run([exe], capture_output=True, text=True)
     assert out.returncode == 0 and "usage" in out.stdout
+
+
+def test_noalloc_array_holds_its_documented_maximum():
+    """The no-alloc entry point's fixed array must hold its largest documented
+    instance (2,048 points, N = 24): the size check comes before any device
+    call, so without a GPU that size gets past it (and fails only on the
+    device), while one point or one neighbour more is a capacity error."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present (the GPU suite runs these sizes for real)")
+    assert f2m_b200.solve_points_noalloc(8, 8, 2048, 24, 8, 8) not in (f2m_b200.OK,
+                                                                        f2m_b200.ERR_CAPACITY)
+    assert f2m_b200.solve_points_noalloc(8, 8, 2049, 24, 8, 8) == f2m_b200.ERR_CAPACITY
+    assert f2m_b200.solve_points_noalloc(8, 8, 2048, 25, 8, 8) == f2m_b200.ERR_CAPACITY

@@ -34,14 +34,16 @@ def _check_against(r, ref_status, ref_lp, ref_max_rank, lab1, lab2, Do, F, xval)
     assert np.array_equal(r.F, F), "potentials differ from the oracle"
     if ref_status == 0:
         assert r.max_rank == ref_max_rank
-        # x is identical except on the B edges of irregular combs whose Ax=b the
-        # device solved: the solution is the same, its last bits may not be
-        # (the reference takes the rows in its hash map's order)
-        simple = np.isin(xval, (0.0, 0.5, 1.0))
-        assert np.array_equal(r.x[simple], xval[simple])
-        assert np.all(np.abs(r.x - xval) <= AXB_XTOL)
-        exact = np.array_equal(r.x, xval)
-        assert _close(r.lp, ref_lp, LP_RTOL if exact else AXB_LP_RTOL)
+        if r.stats["irr_a"] == 0:
+            assert np.array_equal(r.x, xval)
+            assert _close(r.lp, ref_lp)
+        else:
+            # irregular combs, whose Ax=b the device may have solved: the
+            # solution is the same, its last bits may not be (the reference
+            # takes the rows in its hash map's order), so x agrees to FP32
+            # rounding of a 1e-8 residual and the LP value to 1e-9
+            assert np.all(np.abs(r.x - xval) <= AXB_XTOL)
+            assert _close(r.lp, ref_lp, AXB_LP_RTOL)
 
 
 @pytest.mark.parametrize("name", ["uniform200_n10", "config1_n20", "lattice150_s1_n8",
@@ -105,6 +107,14 @@ def test_duplicates_and_rounding(ctx, oracle):
     _check_against(r, o.status, o.lp, o.max_rank, o.lab1, o.lab2, o.Do, o.F, o.x)
 
 
+def _batch_lp_close(lp, lp_o, st_o, n_irr):
+    """LP values of solved instances: to rounding (1e-12) where every comb is
+    regular, to 1e-9 where an irregular comb's Ax=b ran (see _check_against)."""
+    ok = st_o == 0
+    tol = np.where(n_irr > 0, AXB_LP_RTOL, LP_RTOL)
+    assert np.all(np.abs(lp[ok] - lp_o[ok]) <= tol[ok] * np.abs(lp_o[ok]))
+
+
 def test_batch_matches_oracle(ctx, oracle):
     offs, x, y = synth.config3(seed=5, n_inst=40, hi=1500)
     # two lattice instances go through the host comb stage
@@ -116,8 +126,7 @@ def test_batch_matches_oracle(ctx, oracle):
     out = ctx.solve_batch(offs, x, y, 16, details=True)
     lp_o, st_o, _ = oracle.solve_batch(offs, x, y, 16, threads=os.cpu_count() or 1)
     assert np.array_equal(out["status"], st_o)
-    ok = st_o == 0
-    assert np.all(np.abs(out["lp"][ok] - lp_o[ok]) <= LP_RTOL * np.abs(lp_o[ok]))
+    _batch_lp_close(out["lp"], lp_o, st_o, out["n_irregular"])
 
 
 def test_batch_equals_plain_path(ctx):
@@ -251,12 +260,11 @@ def test_nint_cost_mode_matches_oracle(ctx, oracle):
 def test_nint_batch_matches_oracle(ctx, oracle):
     offs, x, y = synth.config3(seed=8, n_inst=30, hi=1200)
     p = f2m_b200.default_params(cost_mode=1)
-    lp, st = ctx.solve_batch(offs, x, y, 16, params=p)
+    out = ctx.solve_batch(offs, x, y, 16, params=p, details=True)
     lp_o, st_o, _ = oracle.solve_batch(offs, x, y, 16, cost=oracle.COST_NINT,
                                        threads=os.cpu_count() or 1)
-    assert np.array_equal(st, st_o)
-    ok = st_o == 0
-    assert np.all(np.abs(lp[ok] - lp_o[ok]) <= LP_RTOL * np.abs(lp_o[ok]))
+    assert np.array_equal(out["status"], st_o)
+    _batch_lp_close(out["lp"], lp_o, st_o, out["n_irregular"])
 
 
 def test_class_bounds_change_speed_not_results(ctx):
@@ -293,13 +301,13 @@ def test_batch_edge_cases_match_oracle(ctx, oracle):
     offs = np.concatenate([[0], np.cumsum([len(p[0]) for p in parts])]).astype(np.int64)
     X = np.concatenate([p[0] for p in parts])
     Y = np.concatenate([p[1] for p in parts])
-    lp, st = ctx.solve_batch(offs, X, Y, 16)
+    out = ctx.solve_batch(offs, X, Y, 16, details=True)
+    st = out["status"]
     lp_o, st_o, _ = oracle.solve_batch(offs, X, Y, 16, threads=os.cpu_count() or 1)
     assert np.array_equal(st, st_o)
     assert st[7] == f2m_b200.ERR_INPUT
-    ok = st_o == 0
-    assert ok.sum() == len(parts) - 1
-    assert np.all(np.abs(lp[ok] - lp_o[ok]) <= LP_RTOL * np.abs(lp_o[ok]))
+    assert (st_o == 0).sum() == len(parts) - 1
+    _batch_lp_close(out["lp"], lp_o, st_o, out["n_irregular"])
 
 
 def test_batch_argument_errors(ctx):

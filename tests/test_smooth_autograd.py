@@ -103,10 +103,14 @@ def test_autograd_function_passes_gradcheck(ctx, torch):
     offs = np.array(offs, np.int64)
     xy = torch.tensor(np.stack([np.concatenate(xs), np.concatenate(ys)], 1).astype(np.float64),
                       requires_grad=True)
-    p = f2m_b200.default_smooth_params(tau=1e-2, iters=40)
+    # tau 5e-2: the logistic terms vary on a scale of tau, so the central
+    # difference's O(eps^2 / tau^2) truncation stays well below the tolerance
+    # (at tau 1e-2 it reaches 1e-3 relative); FP32 distance rounding adds
+    # about 3e-8 / eps
+    p = f2m_b200.default_smooth_params(tau=5e-2, iters=40)
     F = _function(torch)
     assert torch.autograd.gradcheck(lambda t: F.apply(t, offs, N, p, ctx), (xy,), eps=eps,
-                                    atol=1e-4, rtol=1e-3)
+                                    atol=2e-4, rtol=2e-3)
     # the upstream gradient reaches the device: d(3 L0 + 0.5 L1)
     L = F.apply(xy, offs, N, p, ctx)
     (3.0 * L[0] + 0.5 * L[1]).backward()
@@ -121,7 +125,12 @@ def test_autograd_function_passes_gradcheck(ctx, torch):
 def test_gradient_at_config4_defaults_vs_central_differences_and_fp64_host(ctx):
     """10,000 FP32 points uniform in [0,1)^2, N = 30, tau = 1e-3, 100 steps:
     central differences (step 1e-4) of the CUDA forward on 128 seeded points
-    (x and y: 256 coordinates), and the FP64 host gradient everywhere."""
+    (x and y: 256 coordinates), and the FP64 host gradient everywhere.
+
+    At tau = 1e-3 a step of 1e-4 moves a logistic argument by up to 0.1, so
+    the central difference carries an O(h^2) truncation of up to about 1%;
+    the same difference at step 2e-4 gives the Richardson extrapolation,
+    which removes that term and must agree to 2e-3."""
     from oracle import oracle as O
     import f2m_b200
     N, h = 30, 1e-4
@@ -130,24 +139,29 @@ def test_gradient_at_config4_defaults_vs_central_differences_and_fp64_host(ctx):
     assert p.tau == TAU and p.iters == 100
     offs = np.array([0, len(x)], np.int64)
     L0, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
-    safe = np.nonzero(_margins(x, y, N) > 3 * h)[0]
+    safe = np.nonzero(_margins(x, y, N) > 6 * h)[0]  # both steps keep the graph
     rng = np.random.default_rng(128)
     pts = rng.choice(safe, 128, replace=False)
-    worst = 0.0
+
+    def central(arr, i, hh):
+        pp, mm = arr.copy(), arr.copy()
+        pp[i] = np.float32(arr[i] + hh)
+        mm[i] = np.float32(arr[i] - hh)
+        xp, yp = (pp, y) if arr is x else (x, pp)
+        xm, ym = (mm, y) if arr is x else (x, mm)
+        Lp = ctx.smoothed_bound(offs, xp, yp, N, params=p)[0]
+        Lm = ctx.smoothed_bound(offs, xm, ym, N, params=p)[0]
+        half = (float(pp[i]) - float(mm[i])) / 2  # the FP32 step actually taken
+        return (Lp - Lm) / (2 * half), half
+
     for i in pts:
         for arr, g in ((x, gx), (y, gy)):
-            pp, mm = arr.copy(), arr.copy()
-            pp[i] = np.float32(arr[i] + h)
-            mm[i] = np.float32(arr[i] - h)
-            step = float(pp[i]) - float(mm[i])
-            xp, yp = (pp, y) if arr is x else (x, pp)
-            xm, ym = (mm, y) if arr is x else (x, mm)
-            Lp = ctx.smoothed_bound(offs, xp, yp, N, params=p)[0]
-            Lm = ctx.smoothed_bound(offs, xm, ym, N, params=p)[0]
-            fd = (Lp - Lm) / step
-            err = abs(fd - float(g[i])) / max(1.0, abs(float(g[i])))
-            worst = max(worst, err)
-            assert err <= 5e-3, (int(i), fd, float(g[i]))
+            f1, s1 = central(arr, i, h)
+            f2, s2 = central(arr, i, 2 * h)
+            rich = (s2 * s2 * f1 - s1 * s1 * f2) / (s2 * s2 - s1 * s1)
+            scale = max(1.0, abs(float(g[i])))
+            assert abs(f1 - float(g[i])) <= 2e-2 * scale, (int(i), f1, float(g[i]))
+            assert abs(rich - float(g[i])) <= 2e-3 * scale, (int(i), rich, f1, float(g[i]))
     # FP64 host gradient of the same computation, every coordinate
     Lo, dx, dy, _ = O.smooth_bound(x, y, N, tau=p.tau, iters=p.iters, omega=p.damping,
                                    newton_max=p.newton_max, grad=True)

@@ -1,7 +1,7 @@
 """The node gradient of cuda_get_Nodes_grad_R (graph_cuda_grad.hpp:65-84) keeps
 the three smallest reduced costs with a compare chain: `if (v < v0) ...;
 if (v < v1) ...; if (v < v2) ...`.  On the device that chain runs as
-`top3_insert` (f2m_b200/csrc/f2m_device.cuh): two FP64 compares and selects,
+`top3_insert` (f2m_b200/csrc/f2m_device.cuh): three FP64 compares and selects,
 used while the first value is below the 1e6 sentinels (the triple then stays
 sorted).  This test compiles `top3_insert` and `half_grad` for the host with
 the system C++ compiler and compares them with the reference's chain, bit for
