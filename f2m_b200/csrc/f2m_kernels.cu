@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include "f2m_device.cuh"
 #include "f2m_internal.h"
@@ -1413,11 +1414,22 @@ int solve_class_of(int32_t n) {
     return kNumClasses - 1;
 }
 
+// Shared memory of one solver CTA: the device's opt-in limit, or less when
+// F2M_SOLVE_SMEM_KB asks for it (read once per process).  What the CTA does
+// not take stays L1 cache, which then holds the list slices that did not fit
+// in shared memory (they are read from global memory every Jacobi step).
 static size_t smem_per_block() {
+    static int cap_kb = -1;
+    if (cap_kb < 0) {
+        const char* e = getenv("F2M_SOLVE_SMEM_KB");
+        cap_kb = e ? atoi(e) : 0;
+    }
     int dev = 0, v = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    return (size_t)v;
+    size_t bytes = (size_t)v;
+    if (cap_kb > 0 && (size_t)cap_kb * 1024 < bytes) bytes = (size_t)cap_kb * 1024;
+    return bytes;
 }
 
 static int team_bytes_of(int team, int teams) {
