@@ -356,6 +356,55 @@ static __device__ __noinline__ int axb_solve(const AxbRows& S, double* Aj, doubl
     return 0;
 }
 
+// Potentials H = F/2 read from the saved F (halving is exact).
+struct HalfF {
+    const double* F;
+    __device__ __forceinline__ double operator[](int64_t i) const { return 0.5 * F[i]; }
+};
+
+// Sums of the primal over nodes (graph_cuda.cu:135-147, graph_tour.hpp:142-184).
+struct PrimalSums {
+    double lp = 0.0, dual_neg = 0.0, fsum = 0.0;
+    long long maxr = -1, viol = 0;
+};
+// The primal of node v's slots: x = 1 on A edges, 1/2 on B edges -- or, with
+// axb, the Ax=b value when the edge's larger-root comb is irregular (every
+// edge of a comb enters graph::X, whatever its value) -- its code per slot
+// for the host, OVAL = sum x*Do and MAX edge rank over the edges whose other
+// end is the higher id, the degree check (graph_tour.hpp:142-163) and the
+// FP64 dual bound's terms.  lab/irr: comb root per node, irregular flag per
+// root (read only with axb).
+template <class HP, class LP>
+__device__ __forceinline__ void primal_node(const Batch& B, const Inst& I, HP H, LP lab, LP irr, bool axb,
+                                            int v, double porog, PrimalSums& ps) {
+    const int64_t r0 = I.row[v], r1 = I.row[v + 1];
+    const double hv = H[v];
+    ps.fsum += 2.0 * hv;
+    float degsum = 0.0f;
+    bool any = false;
+    for (int64_t a = r0; a < r1; ++a) {
+        const Slot s = I.slot[a];
+        const double d = red_d(s, v, H, hv);
+        double x = (d < porog) ? ((d > -porog) ? 0.5 : 1.0) : 0.0;
+        uint8_t code = (uint8_t)(x == 1.0 ? 2 : (x == 0.5 ? 1 : 0));
+        if (axb && code == 1) {
+            const int l1 = lab[v], l2 = lab[s.nbr];
+            const int c = (l2 == INT_MAX) ? l1 : (l1 == INT_MAX ? l2 : ::max(l1, l2));
+            if (c != INT_MAX && irr[c]) { x = (double)B.xval[a]; code = 3; }
+        }
+        B.xcode[a] = code;
+        const bool in_x = (x != 0.0) || code == 3;
+        degsum += (float)x;
+        any |= in_x;
+        if (s.nbr > v) {
+            ps.lp += x * B.s_cost[a];
+            ps.dual_neg += fmin(0.0, d);
+            if (in_x) ps.maxr = ::max(ps.maxr, (long long)::min((int)(a - r0), B.mirror[a]));
+        }
+    }
+    if (any && !(degsum > 2.0f - 1e-2f && degsum < 2.0f + 1e-2f)) ps.viol++;
+}
+
 // Doubles of scratch one comb needs: its member list (m ints) and its system.
 __device__ __forceinline__ long long axb_comb_doubles(long long m, long long z) {
     return (m + 1) / 2 + 1 + axb_scratch_doubles(m, z);

@@ -14,6 +14,9 @@ namespace f2m {
 // Internal status: the instance needs the host comb solve (Ax=b) because at
 // least one comb violates 2A+B=4 (comb_thread.cpp:180-195).
 constexpr int32_t kNeedsHost = 100;
+// Internal status between the solver and k_axb: the instance has irregular
+// combs whose Ax=b the device solves next (comb_thread.cpp:272-304).
+constexpr int32_t kNeedsAxb = 101;
 
 // One CSR slot as the solver reads it: normalised cost D and neighbour id.
 // `aux` holds the slot's original position in its node's list (the edge's
@@ -93,6 +96,8 @@ struct Batch {
     uint16_t* efN;          // [S] active-set arena: neighbour
     uint8_t* xcode;         // [S] 0, 1 (= 1/2), 2 (= 1), 3 (= xval: an Ax=b solution)
     float* xval;            // [S] x of the B edges of combs solved by Ax=b on the device
+    int32_t* clab;          // [n_total] comb root of each node (INT_MAX outside combs), for k_axb
+    int32_t* cirr;          // [n_total] 1 at the root of an irregular comb, for k_axb
     double* selD;           // [S] SELL-32 slices that do not fit in shared memory: D
     uint16_t* selW;         // [S] ... neighbour word; instance b owns sel_stride * offs[b] ..
     int64_t sel_stride;     //     sel_stride * offs[b+1] (S / n_total entries per point)
@@ -178,6 +183,9 @@ cudaError_t launch_edge_order(const Batch& B, int b, int V, int64_t S, const Edg
 cudaError_t launch_fp64_probe(int kind, int blocks, int iters, double* out, cudaStream_t s);
 double fp64_probe_ops(int kind, int blocks, int iters);
 cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches);
+// Ax=b of the irregular combs and the primal of every instance the solver
+// left with status kNeedsAxb (one CTA per instance of the batch).
+cudaError_t launch_axb(const Batch& B, const DevParams& P, cudaStream_t s, int64_t* launches);
 cudaError_t launch_knn(const Batch& B, int64_t* scan_scratch, cudaStream_t s, int64_t* launches);
 cudaError_t launch_graph(const Batch& B, int64_t* deg_scratch, int64_t* scan_scratch,
                          cudaStream_t s, int64_t* launches);

@@ -22,6 +22,8 @@
 #include <stdint.h>
 #include <stdlib.h>
 
+#include <algorithm>
+
 #include "f2m_device.cuh"
 #include "f2m_internal.h"
 
@@ -1105,46 +1107,6 @@ struct Solver {
         }
         return M_;
     }
-    // comb::solve_AxB (comb_thread.cpp:272-304) for every irregular comb of
-    // the instance, on the device: a thread per comb (roots r = tid, tid +
-    // TEAM, ...), its system in the instance's part of the global slice arena
-    // (free once the descent is over).  The rows are the comb's nodes in
-    // ascending id (the reference takes them in its hash map's order; the
-    // solution does not depend on the order, its last bits may).  Each B edge
-    // takes x (as FP32, as comb::XB holds it) from the comb the host applies
-    // last: graph::X is filled comb by comb in root order, so the comb with
-    // the larger root of the edge's two ends.  Returns false -- the instance
-    // then goes to the host stage, which also runs the repair loop
-    // (graph_cuda.cu:69-126) -- when a system does not converge within 900
-    // steps (the reference allows 999: near that limit the order could
-    // decide) or the arena cannot hold the systems.
-    __device__ bool axb_irregular(const int* irr, const int* lab, double porog) {
-        const int V = I.V;
-        long long need = 0;
-        for (int r = T.tid; r < V; r += TEAM) {
-            if (lab[r] != r || !irr[r]) continue;
-            long long m = 0, z = 0;
-            for (int u = 0; u < V; ++u)
-                if (lab[u] == r) { m++; z += count_b(I.slot, I.row, Hc, u, porog); }
-            need += axb_comb_doubles(m, z);
-        }
-        int total = 0;  // (a thread's share is clamped so that the team sum fits an int)
-        const int off = T.excl_scan((int)::min(need, (long long)1 << 20), &total);
-        if (total > M.gcap) return false;  // team-uniform
-        int bad = need >= ((long long)1 << 20) ? 1 : 0;
-        double* w = M.gsD + off;
-        for (int r = T.tid; r < V && !bad; r += TEAM) {
-            if (lab[r] != r || !irr[r]) continue;
-            int* mem = reinterpret_cast<int*>(w);
-            int m = 0, z = 0;
-            for (int u = 0; u < V; ++u)
-                if (lab[u] == r) { mem[m++] = u; z += count_b(I.slot, I.row, Hc, u, porog); }
-            double* sys = w + (m + 1) / 2 + 1;
-            w += axb_comb_doubles(m, z);
-            bad = axb_comb(I.slot, I.row, row0, B.mirror, Hc, lab, mem, m, z, r, porog, sys, B.xval);
-        }
-        return T.sum_ll(bad) == 0;
-    }
     // Comb extraction (graph_cuda_comb.hpp:415-475), the device comb check and
     // the primal; writes the per-node state for the host and the results.
     __device__ void combs_and_primal(int b, double M_, bool accumulate) {
@@ -1215,42 +1177,24 @@ struct Solver {
             if (lab[v] == v) { nc++; ni += irr[v]; }
         nc = T.sum_ll(nc);
         ni = T.sum_ll(ni);
-        // irregular combs: Ax=b on the device (the first solve only; after a
-        // repair shift the host driver runs the comb stage itself)
-        const bool solved = (ni == 0) || (!accumulate && axb_irregular(irr, lab, porog));
-        // primal (graph_cuda.cu:135-147): x = 1 on A edges, 1/2 on the B edges
-        // of regular combs, the Ax=b solution on those of irregular ones;
-        // OVAL = sum x*Do, MAX edge rank (graph_tour.hpp:165-184)
-        double lp = 0.0, dual_neg = 0.0, fsum = 0.0;
-        long long maxr = -1, viol = 0;
-        for (int v = T.tid; v < V; v += TEAM) {
-            const int64_t r0 = I.row[v], r1 = I.row[v + 1];
-            const double hv = Hc[v];
-            fsum += 2.0 * hv;
-            float degsum = 0.0f;
-            bool any = false;
-            for (int64_t a = r0; a < r1; ++a) {
-                const Slot s = I.slot[a];
-                const double d = red_d(s, v, Hc, hv);
-                double x = (d < porog) ? ((d > -porog) ? 0.5 : 1.0) : 0.0;
-                uint8_t code = (uint8_t)(x == 1.0 ? 2 : (x == 0.5 ? 1 : 0));
-                if (ni > 0 && solved && code == 1) {
-                    const int l1 = lab[v], l2 = lab[s.nbr];
-                    const int c = (l2 == INT_MAX) ? l1 : (l1 == INT_MAX ? l2 : ::max(l1, l2));
-                    if (c != INT_MAX && irr[c]) { x = (double)B.xval[a]; code = 3; }
-                }
-                B.xcode[a] = code;
-                const bool in_x = (x != 0.0) || code == 3;  // every comb edge enters graph::X
-                degsum += (float)x;
-                any |= in_x;
-                if (s.nbr > v) {
-                    lp += x * B.s_cost[a];
-                    dual_neg += fmin(0.0, d);
-                    if (in_x) maxr = ::max(maxr, (long long)::min((int)(a - r0), B.mirror[a]));
-                }
+        // irregular combs of the first solve: k_axb, launched after this
+        // kernel, solves their Ax=b on the device and redoes the primal from
+        // the comb labels saved here (a separate kernel keeps the system
+        // solver's registers out of this one).  After a repair shift the host
+        // driver runs the comb stage itself.
+        const bool axb = ni > 0 && !accumulate;
+        if (axb)
+            for (int v = T.tid; v < V; v += TEAM) {
+                B.clab[I.base + v] = lab[v];
+                B.cirr[I.base + v] = irr[v];
             }
-            if (any && !(degsum > 2.0f - 1e-2f && degsum < 2.0f + 1e-2f)) viol++;
-        }
+        // primal (graph_cuda.cu:135-147): x = 1 on A edges, 1/2 on the B edges
+        // of regular combs; OVAL = sum x*Do, MAX edge rank (graph_tour.hpp:165-184)
+        PrimalSums ps;
+        for (int v = T.tid; v < V; v += TEAM)
+            primal_node(B, I, Hc, (const int*)nullptr, (const int*)nullptr, false, v, porog, ps);
+        double lp = ps.lp, dual_neg = ps.dual_neg, fsum = ps.fsum;
+        long long maxr = ps.maxr, viol = ps.viol;
         lp = T.sum(lp);
         dual_neg = T.sum(dual_neg);
         fsum = T.sum(fsum);
@@ -1271,7 +1215,7 @@ struct Solver {
             B.max_grad[b] = M_;
             B.dual[b] = dmin * (-fsum + dual_neg);
             if (capped) { B.status[b] = F2M_ERR_NOT_CONVERGED; B.lp[b] = NAN; }
-            else if (!solved) { B.status[b] = kNeedsHost; B.lp[b] = NAN; }
+            else if (ni > 0) { B.status[b] = axb ? kNeedsAxb : kNeedsHost; B.lp[b] = NAN; }
             else { B.status[b] = F2M_OK; B.lp[b] = lp; }
         }
         T.sync();
@@ -1329,6 +1273,91 @@ __global__ void __launch_bounds__(TEAM* TEAMS) k_solve(Batch B, DevParams P, con
         }
         S.combs_and_primal(b, Mg, REFIT);
     }
+}
+
+/* ------------------------------------------------------------------ */
+/* k_axb: Ax=b of irregular combs, then the primal                      */
+/* ------------------------------------------------------------------ */
+// comb::solve_AxB (comb_thread.cpp:272-304) for every irregular comb of an
+// instance the solver left with status kNeedsAxb, on the device: a thread
+// per comb (roots r = tid, tid + kAxT, ...), its system in the instance's
+// part of the global slice arena (free once the descent is over).  The rows
+// are the comb's nodes in ascending id (the reference takes them in its hash
+// map's order; the solution does not depend on the order, its last bits
+// may).  Each B edge takes x (as FP32, as comb::XB holds it) from the comb
+// the host applies last: graph::X is filled comb by comb in root order, so
+// the comb with the larger root of the edge's two ends.  When a system does
+// not converge within 900 steps (the reference allows 999: near that limit
+// the order could decide) or the arena cannot hold the systems, the instance
+// goes to the host stage (kNeedsHost), which also runs the repair loop
+// (graph_cuda.cu:69-126); otherwise the primal is redone with the Ax=b
+// values and the instance is solved.  The potentials come from the saved F.
+constexpr int kAxT = 256;
+__global__ void __launch_bounds__(kAxT) k_axb(Batch B, DevParams P) {
+    const int b = blockIdx.x;
+    if (B.status[b] != kNeedsAxb) return;
+    __shared__ int swarp[kAxT / 32 + 1];
+    __shared__ double sred[kAxT / 32];
+    __shared__ long long sredl[kAxT / 32];
+    const Inst I = make_inst(B, b);
+    const int V = I.V;
+    const double porog = P.porog;
+    const int64_t row0 = I.row[0];
+    const HalfF H{B.F + I.base};
+    const int* lab = B.clab + I.base;
+    const int* irr = B.cirr + I.base;
+    long long need = 0;
+    for (int r = threadIdx.x; r < V; r += kAxT) {
+        if (lab[r] != r || !irr[r]) continue;
+        long long m = 0, z = 0;
+        for (int u = 0; u < V; ++u)
+            if (lab[u] == r) { m++; z += count_b(I.slot, I.row, H, u, porog); }
+        need += axb_comb_doubles(m, z);
+    }
+    int total = 0;  // (a thread's share is clamped so that the block sum fits an int)
+    const int off = block_excl_scan<kAxT>((int)::min(need, (long long)1 << 20), swarp, &total);
+    const int64_t p0 = B.offs[b], p1 = B.offs[b + 1];
+    const long long gcap = ::min((long long)(B.sel_stride * (p1 - p0)), (long long)1 << 29);
+    long long bad = (need >= ((long long)1 << 20) || total > gcap) ? 1 : 0;
+    if (total <= gcap) {
+        double* w = B.selD + B.sel_stride * p0 + off;
+        for (int r = threadIdx.x; r < V && !bad; r += kAxT) {
+            if (lab[r] != r || !irr[r]) continue;
+            int* mem = reinterpret_cast<int*>(w);
+            int m = 0, z = 0;
+            for (int u = 0; u < V; ++u)
+                if (lab[u] == r) { mem[m++] = u; z += count_b(I.slot, I.row, H, u, porog); }
+            double* sys = w + (m + 1) / 2 + 1;
+            w += axb_comb_doubles(m, z);
+            bad = axb_comb(I.slot, I.row, row0, B.mirror, H, lab, mem, m, z, r, porog, sys, B.xval);
+        }
+    }
+    if (block_sum_ll<kAxT>(bad, sredl) != 0) {
+        if (threadIdx.x == 0) { B.status[b] = kNeedsHost; B.lp[b] = NAN; }
+        return;
+    }
+    PrimalSums ps;  // __syncthreads inside the sum above orders the xval writes
+    for (int v = threadIdx.x; v < V; v += kAxT) primal_node(B, I, H, lab, irr, true, v, porog, ps);
+    const double lp = block_sum<kAxT>(ps.lp, sred);
+    const double dual_neg = block_sum<kAxT>(ps.dual_neg, sred);
+    const double fsum = block_sum<kAxT>(ps.fsum, sred);
+    const long long maxr = block_max_ll<kAxT>(ps.maxr, sredl);
+    const long long viol = block_sum_ll<kAxT>(ps.viol, sredl);
+    if (threadIdx.x == 0) {
+        const double dmin = __longlong_as_double((long long)B.dmin_bits[b]);
+        B.max_rank[b] = (int32_t)maxr;
+        B.deg_viol[b] = (int32_t)viol;
+        B.dual[b] = dmin * (-fsum + dual_neg);
+        B.status[b] = F2M_OK;
+        B.lp[b] = lp;
+    }
+}
+
+cudaError_t launch_axb(const Batch& B, const DevParams& P, cudaStream_t s, int64_t* launches) {
+    if (B.n_inst <= 0) return cudaSuccess;
+    k_axb<<<B.n_inst, kAxT, 0, s>>>(B, P);
+    ++*launches;
+    return cudaGetLastError();
 }
 
 /* ------------------------------------------------------------------ */
@@ -1414,28 +1443,43 @@ int solve_class_of(int32_t n) {
     return kNumClasses - 1;
 }
 
-// Shared memory of one solver CTA: the device's opt-in limit, or less when
-// F2M_SOLVE_SMEM_KB asks for it (read once per process).  What the CTA does
-// not take stays L1 cache, which then holds the list slices that did not fit
-// in shared memory (they are read from global memory every Jacobi step).
-static size_t smem_per_block() {
-    static int cap_kb = -1;
-    if (cap_kb < 0) {
-        const char* e = getenv("F2M_SOLVE_SMEM_KB");
-        cap_kb = e ? atoi(e) : 0;
-    }
+// Shared memory of the solver CTAs.  A CTA does not take the whole opt-in
+// limit: what it leaves stays L1 cache, which then holds the list slices
+// that did not fit in shared memory (read from global memory every Jacobi
+// step) and the slot records the partitions scan.  On the batched workload
+// a 132 KB CTA (124 KB of L1) solves faster than a 227 KB one (about 5%).
+// F2M_SOLVE_SMEM_KB overrides the target (read once per process; 0 = the
+// whole opt-in limit).  A launch whose largest instance needs more than the
+// target for its fixed part (potentials, slice tables) takes what it needs.
+constexpr int kSolveSmemKB = 132;
+static size_t smem_optin() {
     int dev = 0, v = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    size_t bytes = (size_t)v;
-    if (cap_kb > 0 && (size_t)cap_kb * 1024 < bytes) bytes = (size_t)cap_kb * 1024;
-    return bytes;
+    return (size_t)v;
 }
+static size_t smem_target() {
+    static int kb = -1;
+    if (kb < 0) {
+        const char* e = getenv("F2M_SOLVE_SMEM_KB");
+        kb = e ? atoi(e) : kSolveSmemKB;
+        if (kb < 0) kb = 0;
+    }
+    const size_t optin = smem_optin();
+    return (kb > 0 && (size_t)kb * 1024 < optin) ? (size_t)kb * 1024 : optin;
+}
+template <int TEAM, int TEAMS>
+static size_t solve_static_smem() {
+    return sizeof(double) * TEAMS * (TEAM / 32) * 2 + sizeof(int) * TEAMS * (TEAM / 32 + 5) + 64;
+}
+// dynamic bytes of a CTA of TEAMS teams out of `total` shared memory, and
+// each team's share
+static size_t dyn_of(size_t total, size_t stat) { return (total - stat) & ~(size_t)255; }
+static int team_share(size_t dyn, int teams) { return (int)((dyn / teams) & ~(size_t)15); }
 
-static int team_bytes_of(int team, int teams) {
+static int team_bytes_of(int team, int teams) {  // at the opt-in limit (class capacities)
     const size_t stat = sizeof(double) * teams * (team / 32) * 2 + sizeof(int) * teams * (team / 32 + 5) + 64;
-    const size_t dyn = (smem_per_block() - stat) & ~(size_t)255;
-    return (int)((dyn / teams) & ~(size_t)15);
+    return team_share(dyn_of(smem_optin(), stat), teams);
 }
 static int class_capacity(int c) {
     const int tb = team_bytes_of(kClasses[c].team, kClasses[c].teams);
@@ -1450,9 +1494,14 @@ static int class_capacity(int c) {
 template <int TEAM, int TEAMS, bool R>
 static cudaError_t launch_one(const Batch& B, const DevParams& P, const int32_t* items, int n_items,
                               int32_t* queue, int vcap, cudaStream_t s, int64_t* launches) {
-    const size_t stat = sizeof(double) * TEAMS * (TEAM / 32) * 2 + sizeof(int) * TEAMS * (TEAM / 32 + 5) + 64;
-    const size_t dyn = (smem_per_block() - stat) & ~(size_t)255;
-    const int team_bytes = team_bytes_of(TEAM, TEAMS);
+    const size_t stat = solve_static_smem<TEAM, TEAMS>();
+    const size_t optin = smem_optin();
+    // the target, or what the largest instance's fixed part needs (with 4 KB
+    // of slice cache per team), if more
+    const size_t need = stat + 256 + (size_t)TEAMS * (team_fixed_bytes(vcap) + 16 + 4096);
+    const size_t total = std::min(optin, std::max(smem_target(), need));
+    const size_t dyn = dyn_of(total, stat);
+    const int team_bytes = team_share(dyn, TEAMS);
     if (team_fixed_bytes(vcap) > (size_t)team_bytes) return cudaErrorInvalidConfiguration;
     cudaError_t e = cudaFuncSetAttribute(k_solve<TEAM, TEAMS, R>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
@@ -1463,8 +1512,8 @@ static cudaError_t launch_one(const Batch& B, const DevParams& P, const int32_t*
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<TEAM, TEAMS, R>, TEAM * TEAMS, dyn);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int grid = sms * per_sm;
-    const int need = (n_items + TEAMS - 1) / TEAMS;
-    if (grid > need) grid = need;
+    const int need_ctas = (n_items + TEAMS - 1) / TEAMS;
+    if (grid > need_ctas) grid = need_ctas;
     if ((e = cudaMemsetAsync(queue, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
     k_solve<TEAM, TEAMS, R><<<grid, TEAM * TEAMS, dyn, s>>>(B, P, items, n_items, queue, vcap, team_bytes);
     ++*launches;

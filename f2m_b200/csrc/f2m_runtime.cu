@@ -278,6 +278,8 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
     B.efN = A.take<uint16_t>(S);
     B.xcode = A.take<uint8_t>(S);
     B.xval = A.take<float>(S);
+    B.clab = A.take<int32_t>(n);
+    B.cirr = A.take<int32_t>(n);
     B.selD = A.take<double>(S);
     B.selW = A.take<uint16_t>(S);
     B.sel_stride = S / n;
@@ -830,6 +832,8 @@ f2m_status launch_classes(f2m_ctx* ctx, DevCall& C, const f2m_params& prm) {
         F2M_CUDA(cudaEventRecord(ctx->join[c], ctx->aux[c]));
         F2M_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[c], 0));
     }
+    // irregular combs of the first solve: Ax=b and the primal on the device
+    F2M_CUDA(launch_axb(C.B, P, ctx->stream, &ctx->launches));
     return F2M_OK;
 }
 
@@ -2487,7 +2491,8 @@ extern "C" f2m_status f2m_solve_points_noalloc(const double* d_x, const double* 
     if (launch_prep(B, s, &launches) != cudaSuccess || launch_knn(B, scan, s, &launches) != cudaSuccess ||
         launch_graph(B, deg, scan, s, &launches) != cudaSuccess ||
         launch_solve_class(solve_class_of(n), B, to_dev(prm), ord, 1, B.queue, std::max<int32_t>(n, 4), s,
-                           &launches) != cudaSuccess)
+                           &launches) != cudaSuccess ||
+        launch_axb(B, to_dev(prm), s, &launches) != cudaSuccess)
         return F2M_ERR_CUDA;
     k_noalloc_finish<<<1, 32, 0, s>>>(B.status, B.lp, d_status, d_lp);
     if (cudaGetLastError() != cudaSuccess) return F2M_ERR_CUDA;
