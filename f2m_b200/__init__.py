@@ -92,7 +92,7 @@ EXPORTS = [
     "f2m_solve_points_noalloc", "f2m_default_smooth_params", "f2m_smoothed_bound_fwd",
     "f2m_smoothed_bound_bwd", "f2m_smooth_max_nodes", "f2m_knn", "f2m_set_class_bounds",
     "f2m_get_class_bounds", "f2m_solve_graph", "f2m_solve_points_from", "f2m_fp64_rate",
-    "f2m_smoothed_bound_bwd_edges",
+    "f2m_smoothed_bound_bwd_edges", "f2m_set_solver_smem_kb", "f2m_get_solver_smem_kb",
 ]
 
 _lib = None
@@ -145,6 +145,8 @@ def lib():
         L.f2m_smooth_max_nodes.restype = i32
         L.f2m_set_class_bounds.argtypes = [vp]
         L.f2m_get_class_bounds.argtypes = [vp]
+        L.f2m_set_solver_smem_kb.argtypes = [i32]
+        L.f2m_get_solver_smem_kb.restype = i32
         _lib = L
     return _lib
 
@@ -171,16 +173,30 @@ def get_class_bounds():
     return [int(v) for v in b]
 
 
+def set_solver_smem_kb(kb):
+    """Shared memory (KB) a CTA of the batched solver takes; 0 = all of it."""
+    s = lib().f2m_set_solver_smem_kb(int(kb))
+    if s != OK:
+        raise F2MError(s, f"solver shared memory {kb} KB rejected")
+
+
+def get_solver_smem_kb():
+    return int(lib().f2m_get_solver_smem_kb())
+
+
 def load_tuning(path=None):
-    """Apply the class bounds recorded by f2m_b200.autotune (default: the
-    committed f2m_b200/tuned_classes.json); returns them, or None."""
+    """Apply the class bounds (and the solver's shared-memory target, when
+    recorded) of f2m_b200.autotune (default: the committed
+    f2m_b200/tuned_classes.json); returns the bounds, or None."""
     import json
     path = path or os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_classes.json")
     if not os.path.exists(path):
         return None
-    bounds = json.load(open(path))["bounds"]
-    set_class_bounds(bounds)
-    return bounds
+    rec = json.load(open(path))
+    set_class_bounds(rec["bounds"])
+    if "smem_kb" in rec:
+        set_solver_smem_kb(rec["smem_kb"])
+    return rec["bounds"]
 
 
 def default_smooth_params(**overrides):

@@ -202,6 +202,8 @@ int solve_num_classes();
 int solve_class_of(int32_t n);
 int solve_set_bounds(const int32_t* max_n);  // 3 increasing bounds; -1 if rejected
 void solve_get_bounds(int32_t* max_n);
+int solve_set_smem_kb(int kb);                // shared-memory target of a solver CTA (0 = all)
+int solve_get_smem_kb();
 // Smoothed-bound batch (f2m_smooth.cu).  Node g of instance b is offs[b] +
 // local id; neighbour ids in nbr are local; slots are global (row).
 struct SmoothBatch {

@@ -1449,7 +1449,8 @@ int solve_class_of(int32_t n) {
 // step) and the slot records the partitions scan.  On the batched workload
 // a 132 KB CTA (124 KB of L1) solves faster than a 227 KB one (about 5%).
 // F2M_SOLVE_SMEM_KB overrides the target (read once per process; 0 = the
-// whole opt-in limit).  A launch whose largest instance needs more than the
+// whole opt-in limit; f2m_set_solver_smem_kb sets it at run time, as the
+// autotuner does).  A launch whose largest instance needs more than the
 // target for its fixed part (potentials, slice tables) takes what it needs.
 constexpr int kSolveSmemKB = 132;
 static size_t smem_optin() {
@@ -1458,13 +1459,22 @@ static size_t smem_optin() {
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     return (size_t)v;
 }
-static size_t smem_target() {
-    static int kb = -1;
-    if (kb < 0) {
+static int g_smem_kb = -1;  // process-wide target (solve_set_smem_kb); -1: not read yet
+int solve_get_smem_kb() {
+    if (g_smem_kb < 0) {
         const char* e = getenv("F2M_SOLVE_SMEM_KB");
-        kb = e ? atoi(e) : kSolveSmemKB;
-        if (kb < 0) kb = 0;
+        g_smem_kb = e ? atoi(e) : kSolveSmemKB;
+        if (g_smem_kb < 0) g_smem_kb = 0;
     }
+    return g_smem_kb;
+}
+int solve_set_smem_kb(int kb) {
+    if (kb < 0 || kb > 4096) return -1;
+    g_smem_kb = kb;
+    return 0;
+}
+static size_t smem_target() {
+    const int kb = solve_get_smem_kb();
     const size_t optin = smem_optin();
     return (kb > 0 && (size_t)kb * 1024 < optin) ? (size_t)kb * 1024 : optin;
 }

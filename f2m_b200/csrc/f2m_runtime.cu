@@ -1833,6 +1833,10 @@ f2m_status f2m_set_class_bounds(const int32_t* max_nodes) {
     return solve_set_bounds(max_nodes) == 0 ? F2M_OK : F2M_ERR_INPUT;
 }
 void f2m_get_class_bounds(int32_t* max_nodes) { solve_get_bounds(max_nodes); }
+f2m_status f2m_set_solver_smem_kb(int32_t kb) {
+    return solve_set_smem_kb(kb) == 0 ? F2M_OK : F2M_ERR_INPUT;
+}
+int32_t f2m_get_solver_smem_kb(void) { return solve_get_smem_kb(); }
 
 }  // extern "C"
 

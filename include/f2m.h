@@ -318,6 +318,14 @@ int32_t f2m_smooth_max_nodes(void);
  * increasing or a class's shared memory cannot hold an instance that size. */
 f2m_status f2m_set_class_bounds(const int32_t* max_nodes); /* 3 values */
 void f2m_get_class_bounds(int32_t* max_nodes);
+/* Shared memory a CTA of the batched solver takes, in KB (no reference
+ * counterpart; process-wide, like the class bounds).  What a CTA leaves
+ * stays L1 cache, which holds the list slices that did not fit in shared
+ * memory; 0 takes the whole opt-in limit.  A launch whose largest instance
+ * needs more for its fixed part takes what it needs.  Default 132 (or
+ * F2M_SOLVE_SMEM_KB); f2m_b200/autotune.py tunes it with the bounds. */
+f2m_status f2m_set_solver_smem_kb(int32_t kb);
+int32_t f2m_get_solver_smem_kb(void);
 
 #ifdef __cplusplus
 }
