@@ -24,6 +24,8 @@
 #include <stdint.h>
 
 
+#include <algorithm>
+
 #include "f2m_device.cuh"
 #include "f2m_internal.h"
 
@@ -1110,6 +1112,62 @@ cudaError_t launch_edge_order(const Batch& B, int b, int V, int64_t S, const Edg
     e = radix_sort(kc, ks, vs, vfree, S, 0, 64, E.tmp, E.tmp_bytes, s, launches, &ks, &vs);
     if (e != cudaSuccess) return e;
     *order = vs;
+    return cudaGetLastError();
+}
+
+/* ------------------------------------------------------------------ */
+/* the result arrays in the reference's edge order                      */
+/* ------------------------------------------------------------------ */
+EdgeExport edge_export_view(void* xout, int64_t E) {
+    EdgeExport X;
+    double* d = static_cast<double*>(xout);
+    X.Do = d;
+    X.D = d + E;
+    X.x = d + 2 * E;
+    int32_t* i = reinterpret_cast<int32_t*>(d + 3 * E);
+    X.ev1 = i;
+    X.ev2 = i + E;
+    X.el1 = i + 2 * E;
+    X.el2 = i + 3 * E;
+    return X;
+}
+
+// Edge e of the order is the slot order[e] of its lower-id endpoint (found
+// by binary search over the instance's row offsets); x follows the slot's
+// primal code (graph::X, F2M.h:161), the labels the points' labels.
+__global__ void k_export_edges(Batch B, int b, int V, const uint32_t* order, int64_t E, EdgeExport X) {
+    const int64_t base = B.offs[b];
+    const int64_t* row = B.row + base;
+    const int64_t s0 = row[0];
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = s0 + order[e];
+        int lo = 0, hi = V - 1;  // the last node whose list starts at or before a
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (row[mid] <= a) lo = mid; else hi = mid - 1;
+        }
+        const int v = lo;
+        const Slot s = B.slot[a];
+        const int u = s.nbr;
+        const uint8_t c = B.xcode[a];
+        X.ev1[e] = v;
+        X.ev2[e] = u;
+        const bool vlow = B.K[base + v] < B.K[base + u];
+        X.el1[e] = vlow ? v : u;
+        X.el2[e] = vlow ? u : v;
+        X.Do[e] = B.s_cost[a];
+        X.D[e] = s.D;
+        X.x[e] = c == 3 ? (double)B.xval[a] : (c == 2 ? 1.0 : (c == 1 ? 0.5 : 0.0));
+    }
+}
+
+cudaError_t launch_export_edges(const Batch& B, int b, int V, const uint32_t* order, int64_t E,
+                                const EdgeExport& X, cudaStream_t s, int64_t* launches) {
+    if (E <= 0) return cudaSuccess;
+    const int T = 256;
+    const int64_t blocks = std::min<int64_t>((E + T - 1) / T, 148 * 16);
+    k_export_edges<<<(unsigned)blocks, T, 0, s>>>(B, b, V, order, E, X);
+    ++*launches;
     return cudaGetLastError();
 }
 

@@ -171,8 +171,19 @@ struct EdgeSort {
     uint32_t* v2;            // [S]
     void* tmp;               // radix-sort scratch
     size_t tmp_bytes;
+    void* xout;              // [S * 20 bytes] the exported edge arrays (EdgeExport)
 };
 size_t edge_order_temp_bytes(int64_t S);
+// The result arrays of one solved instance in the reference's edge order,
+// written on the device: internal ids of the lower/higher-id endpoint, of
+// the lower/higher-label endpoint, raw and normalised cost, primal x.
+struct EdgeExport {
+    int32_t *ev1, *ev2, *el1, *el2;
+    double *Do, *D, *x;
+};
+EdgeExport edge_export_view(void* xout, int64_t E);
+cudaError_t launch_export_edges(const Batch& B, int b, int V, const uint32_t* order, int64_t E,
+                                const EdgeExport& X, cudaStream_t s, int64_t* launches);
 // The reference's edge order (ascending cost, then emitter, then partner:
 // graph_tour.hpp:28-98) of instance b's edges, each as the offset of its slot
 // in the lower-id endpoint's list (within the instance's slots); the first

@@ -900,11 +900,11 @@ struct Solver {
     __device__ void swap_f() { double* t = Hc; Hc = Hn; Hn = t; }
 
     // grad/2 of the node in lane `lane` of slice s; v = that node (or -1)
-    __device__ __forceinline__ double slice_hgrad(int s, int lane, int& v) const {
+    __device__ __forceinline__ double slice_hgrad(int s, int lane, int& v, double& hv) const {
         const int p = s * 32 + lane;
         v = (p < I.V) ? (int)M.ord[p] : -1;
         const int vv = v < 0 ? (int)M.ord[s * 32] : v;  // padding lanes shadow lane 0
-        const double hv = Hc[vv];
+        hv = Hc[vv];
         const int off = M.soff[s];
         if (off >= 0) {
             const double* Dp = M.eD + off + lane;
@@ -928,8 +928,9 @@ struct Solver {
         const int w = T.tid >> 5, lane = T.tid & 31;
         for (int s = w; s < M.NS; s += WARPS) {
             int v;
-            const double g = slice_hgrad(s, lane, v);
-            if (v >= 0) Hn[v] = (MASKED && B.shift[I.base + v] != 0.0) ? Hc[v] : Hc[v] + g;
+            double hv;
+            const double g = slice_hgrad(s, lane, v, hv);
+            if (v >= 0) Hn[v] = (MASKED && B.shift[I.base + v] != 0.0) ? hv : hv + g;
         }
         wslots += M.hist[256];
         wpad += M.hist[257];
@@ -945,7 +946,8 @@ struct Solver {
         double m = 0.0;
         for (int s = w; s < M.NS; s += WARPS) {
             int v;
-            const double g = slice_hgrad(s, lane, v);
+            double hv;
+            const double g = slice_hgrad(s, lane, v, hv);
             if (v >= 0) m = fmax(m, fabs(g));
         }
         return 2.0 * T.max(m);

@@ -775,6 +775,7 @@ void carve_edge_sort(Arena& A, EdgeSort& E, int64_t S) {
     E.v2 = A.take<uint32_t>(S);
     E.tmp_bytes = edge_order_temp_bytes(S);
     E.tmp = A.take<unsigned char>(E.tmp_bytes);
+    E.xout = A.take<double>((S * 20 + 7) / 8);  // E = S/2 edges x 40 bytes
 }
 
 f2m_status setup_call(f2m_ctx* ctx, DevCall& C, int32_t n_inst, const int64_t* h_offs, int32_t top_k,
@@ -1083,66 +1084,75 @@ f2m_status complete_instance(f2m_ctx* ctx, DevCall& C, int b, const f2m_params& 
     return F2M_OK;
 }
 
-// The primal of an instance whose combs the device found all regular
-// (2A+B = 4 at every comb node, status F2M_OK): then every comb's solution is
-// x = 1/2 on its half edges (comb_thread.cpp solve_simple), which is the
-// device's per-slot code (xcode), so the host comb stage would change
-// nothing.  x, MAX rank, the degree check and the dual bound are taken as
-// complete_instance takes them, and OVAL is summed in edge-id order (the
-// host stage sums in graph::X's hash order; the two agree to rounding);
-// comb counts come from the device.  Used by the points path; the file
-// path keeps the host stage, which also writes the reference's files.
-f2m_status complete_from_device(f2m_ctx* ctx, const DevCall& C, int b, f2m_result& R) {
-    Range rg("f2m complete instance (device combs)");
+// The result of an instance the device completed (every comb regular, or
+// the irregular ones solved by Ax=b, status F2M_OK): the edge arrays in the
+// reference's edge order (graph_tour.hpp:28-98) are written on the device
+// (launch_edge_order, then k_export_edges) and come back in one copy, with
+// the node labels and potentials; OVAL, MAX edge rank, the degree check and
+// the FP64 dual bound are the device's (graph_tour.hpp:142-184; OVAL summed
+// in the solver's order, which agrees with the host stage's hash order to
+// rounding).  The host builds none of the comb stage's structures.  Used by
+// the points path; the file path keeps the host stage, which also writes the
+// reference's files.
+f2m_status export_from_device(f2m_ctx* ctx, const DevCall& C, int b, f2m_result& R) {
+    Range rg("f2m export instance (device)");
+    const Batch& B = C.B;
     HostInst& H = R.H;
-    int64_t base = 0, s0 = 0;
-    int32_t nc = 0, ni = 0;
-    F2M_CUDA(cudaMemcpyAsync(&base, C.B.offs + b, sizeof(base), cudaMemcpyDeviceToHost, ctx->stream));
+    int32_t V = 0, nc = 0, ni = 0, mr = 0, viol = 0;
+    int64_t base = 0;
+    unsigned long long db = 0;
+    double lp = 0, dual = 0;
+    auto small = [&](void* dst, const void* src, size_t n) {
+        return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->stream);
+    };
+    F2M_CUDA(small(&V, B.Vn + b, 4));
+    F2M_CUDA(small(&base, B.offs + b, 8));
+    F2M_CUDA(small(&db, B.dmin_bits + b, 8));
+    F2M_CUDA(small(&nc, B.n_combs + b, 4));
+    F2M_CUDA(small(&ni, B.n_irr + b, 4));
+    F2M_CUDA(small(&mr, B.max_rank + b, 4));
+    F2M_CUDA(small(&viol, B.deg_viol + b, 4));
+    F2M_CUDA(small(&lp, B.lp + b, 8));
+    F2M_CUDA(small(&dual, B.dual + b, 8));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
-    F2M_CUDA(cudaMemcpyAsync(&s0, C.B.row + base, sizeof(s0), cudaMemcpyDeviceToHost, ctx->stream));
-    F2M_CUDA(cudaMemcpyAsync(&nc, C.B.n_combs + b, sizeof(nc), cudaMemcpyDeviceToHost, ctx->stream));
-    F2M_CUDA(cudaMemcpyAsync(&ni, C.B.n_irr + b, sizeof(ni), cudaMemcpyDeviceToHost, ctx->stream));
+    int64_t r0 = 0, r1 = 0;
+    F2M_CUDA(small(&r0, B.row + base, 8));
+    F2M_CUDA(small(&r1, B.row + base + V, 8));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
-    const int64_t S = (int64_t)H.nbr.size();
-    // per-slot codes, and the Ax=b values where the device solved irregular combs
-    const size_t xv_off = ((size_t)S + 15) & ~(size_t)15;
-    F2M_CUDA(ensure_pinned(ctx, xv_off + (ni > 0 ? (size_t)S * sizeof(float) : 0) + 16));
-    F2M_CUDA(cudaMemcpyAsync(ctx->pinned, C.B.xcode + s0, S, cudaMemcpyDeviceToHost, ctx->stream));
-    if (ni > 0)
-        F2M_CUDA(cudaMemcpyAsync(ctx->pinned + xv_off, C.B.xval + s0, S * sizeof(float), cudaMemcpyDeviceToHost,
-                                 ctx->stream));
+    const int64_t S = r1 - r0, E = S / 2;
+    const uint32_t* ord = nullptr;
+    F2M_CUDA(launch_edge_order(B, b, V, S, C.es, &ord, ctx->stream, &ctx->launches));
+    const EdgeExport X = edge_export_view(C.es.xout, E);
+    F2M_CUDA(launch_export_edges(B, b, V, ord, E, X, ctx->stream, &ctx->launches));
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    F2M_CUDA(ensure_pinned(ctx, al(E * 40) + al(V * 12)));
+    char* q = ctx->pinned;
+    F2M_CUDA(small(q, C.es.xout, E * 40));  // Do, D, x, ev1, ev2, el1, el2 back to back
+    double* F = reinterpret_cast<double*>(q + al(E * 40));
+    int32_t* K = reinterpret_cast<int32_t*>(q + al(E * 40) + V * 8);
+    F2M_CUDA(small(F, B.F + base, V * 8));
+    F2M_CUDA(small(K, B.K + base, V * 4));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
-    const uint8_t* xc = reinterpret_cast<const uint8_t*>(ctx->pinned);
-    const float* xv = reinterpret_cast<const float*>(ctx->pinned + xv_off);
-    R.x.assign(H.E, 0.0);
-    std::vector<char> inx(H.E, 0);  // in graph::X (every comb edge is, whatever its value)
-    parallel_for(H.E, [&](int64_t e0, int64_t e1) {
-        for (int64_t e = e0; e < e1; ++e) {
-            const int v = H.ev1[e];
-            const int64_t a = H.row[v] + (H.el1[e] == v ? H.rank1[e] : H.rank2[e]);
-            const uint8_t c = xc[a];
-            R.x[e] = c == 3 ? (double)xv[a] : (c == 2 ? 1.0 : (c == 1 ? 0.5 : 0.0));
-            inx[e] = c != 0;
-        }
+    const EdgeExport P = edge_export_view(q, E);
+    H.V = V;
+    H.E = (int)E;
+    std::memcpy(&H.dmin, &db, sizeof(double));
+    H.label.assign(K, K + V);
+    H.F.assign(F, F + V);
+    H.ev1.resize(E); H.ev2.resize(E); H.el1.resize(E); H.el2.resize(E);
+    H.eDo.resize(E); H.eD.resize(E); R.x.resize(E);
+    parallel_for(E, [&](int64_t e0, int64_t e1) {
+        const size_t n4 = (e1 - e0) * 4, n8 = (e1 - e0) * 8;
+        std::memcpy(H.ev1.data() + e0, P.ev1 + e0, n4);
+        std::memcpy(H.ev2.data() + e0, P.ev2 + e0, n4);
+        std::memcpy(H.el1.data() + e0, P.el1 + e0, n4);
+        std::memcpy(H.el2.data() + e0, P.el2 + e0, n4);
+        std::memcpy(H.eDo.data() + e0, P.Do + e0, n8);
+        std::memcpy(H.eD.data() + e0, P.D + e0, n8);
+        std::memcpy(R.x.data() + e0, P.x + e0, n8);
     });
     R.X.clear();
-    double OVAL = 0;  // graph::getOVAL (graph_tour.hpp:165-184)
-    int mr = 0;
-    std::vector<float> deg(H.V, 0.0f);
-    std::vector<char> has(H.V, 0);
-    for (int e = 0; e < H.E; ++e) {
-        const double x = R.x[e];
-        if (!inx[e]) continue;
-        R.X.emplace(e, x);
-        mr = std::max(mr, std::min(H.rank1[e], H.rank2[e]));
-        OVAL += x * H.eDo[e];
-        deg[H.el1[e]] += (float)x; has[H.el1[e]] = 1;
-        deg[H.el2[e]] += (float)x; has[H.el2[e]] = 1;
-    }
-    int viol = 0;  // graph::check_solution (graph_tour.hpp:142-163)
-    for (int v = 0; v < H.V; ++v)
-        if (has[v] && !(deg[v] > 2.0f - 1e-2f && deg[v] < 2.0f + 1e-2f)) viol++;
-    R.lp = OVAL;
+    R.lp = lp;
     R.max_rank = mr;
     R.status = F2M_OK;
     R.st.repair_steps = 0;
@@ -1150,13 +1160,7 @@ f2m_status complete_from_device(f2m_ctx* ctx, const DevCall& C, int b, f2m_resul
     R.st.irr_b = 0;
     R.st.n_combs = nc;
     R.st.degree_violations = viol;
-    double fsum = 0, neg = 0;  // FP64 dual bound, as complete_instance
-    for (int v = 0; v < H.V; ++v) fsum += H.F[v];
-    for (int e = 0; e < H.E; ++e) {
-        const double d = (H.eD[e] + 0.5 * H.F[H.ev1[e]]) + 0.5 * H.F[H.ev2[e]];
-        neg += std::min(0.0, d);
-    }
-    R.st.dual_value = H.dmin * (-fsum + neg);
+    R.st.dual_value = dual;
     R.st.d_min = H.dmin;
     return F2M_OK;
 }
@@ -1645,15 +1649,18 @@ f2m_status points_call(f2m_ctx* ctx, const double* x, const double* y, const int
         *out = R.release();
         return (f2m_status)st;
     }
-    if ((s = pull_instance(ctx, C, 0, R->H, true))) return s;
-    clk.mark("pull");
-    if ((s = pull_stats(ctx, C, 0, *R))) return s;
     // every comb regular, or the irregular ones solved by Ax=b on the device:
-    // the device's primal stands; otherwise (an Ax=b system that did not
-    // converge, so the repair loop runs) the host comb stage as the
-    // reference runs it
-    if ((s = (st == F2M_OK ? complete_from_device(ctx, C, 0, *R) : complete_instance(ctx, C, 0, prm, *R))))
-        return s;
+    // the device's primal stands and its arrays come back in edge order;
+    // otherwise (an Ax=b system that did not converge, so the repair loop
+    // runs) the host comb stage as the reference runs it
+    if (st == F2M_OK) {
+        if ((s = export_from_device(ctx, C, 0, *R))) return s;
+        clk.mark("export");
+    } else {
+        if ((s = pull_instance(ctx, C, 0, R->H, true))) return s;
+        clk.mark("pull");
+        if ((s = complete_instance(ctx, C, 0, prm, *R))) return s;
+    }
     clk.mark("complete");
     if ((s = pull_stats(ctx, C, 0, *R))) return s;
     R->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
