@@ -297,6 +297,151 @@ __device__ __forceinline__ int qpart_ef_la(const Inst& I, int64_t r0, int v, HP 
     return size;
 }
 
+// qpart_ptr_EF on a node's list copied to shared memory: `pl` holds the list
+// order and `val` the reduced cost of each position.  The loop is qpart_ef's
+// (the Hoare scans, the swaps, which move both arrays, and the threshold
+// sequence), so the final order and count are the same; only the values are
+// read from shared memory instead of three dependent global loads each.
+__device__ inline int qpart_b_vals(uint16_t* pl, double* val, int size, double avg) {
+    int low = 0, high = size - 1, i = low, j = high;
+    for (int pass = 0; i < j && pass <= size; ++pass) {
+        while (i <= high && val[i] <= avg) i++;
+        while (j >= low && val[j] > avg) j--;
+        if (i < j) {
+            const uint16_t t = pl[i]; pl[i] = pl[j]; pl[j] = t;
+            const double u = val[i]; val[i] = val[j]; val[j] = u;
+        }
+    }
+    return j + 1;
+}
+__device__ inline int qpart_ef_vals(uint16_t* pl, double* val, int size, double avg, int ef_min) {
+    if (size < ef_min) return size;
+    constexpr int kLimit = 1 << 20;
+    for (int bump = 0; bump < kLimit;) {
+        const int p = qpart_b_vals(pl, val, size, avg);
+        if (p >= ef_min) return p;
+        double g = INFINITY;
+        bool nan = false;
+        for (int k = 0; k < size; ++k) {
+            nan |= (val[k] != val[k]);
+            if (k >= p) g = fmin(g, val[k]);
+        }
+        avg += 1;
+        ++bump;
+        if (nan) continue;
+        bump_until(avg, bump, g, kLimit);
+    }
+    return size;
+}
+
+// The same partition run by a whole warp.  On finite values the Hoare loop
+// of qpart_b_vals is a fixed pairing: with Lc the number of entries <= avg,
+// its t-th swap exchanges the t-th entry > avg of [0, Lc) (ascending) with
+// the t-th entry <= avg of [Lc, size) (descending), for every t below the
+// number m of entries > avg in [0, Lc), and it returns Lc (a list of one
+// entry is returned as it is: the loop does not run).  Each lane ranks its
+// entries with ballots and moves the ones that swap, so the final order and
+// the count are the serial loop's.  Lists of at most 32 * NC entries in
+// shared memory; every lane of the warp calls it with the same arguments.
+__device__ __forceinline__ int nth_bit(unsigned m, int n) {  // position of the n-th (0-based) set bit
+    int pos = 0;
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1) {
+        const int c = __popc(m & ((1u << w) - 1u));
+        if (n >= c) { n -= c; m >>= w; pos += w; }
+    }
+    return pos;
+}
+template <int NC>
+__device__ __forceinline__ int nth_bit_of(const unsigned (&m)[NC], int n) {
+    int r = -1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const int pc = __popc(m[c]);
+        if (r < 0 && n < pc) r = c * 32 + nth_bit(m[c], n);
+        n -= pc;
+    }
+    return r;
+}
+template <int NC>
+__device__ __forceinline__ int warp_qpart_b_vals(uint16_t* pl, double* val, int size, double avg, int lane) {
+    if (size <= 1) return size;
+    unsigned gt[NC];
+    int G = 0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const int e = c * 32 + lane;
+        gt[c] = __ballot_sync(0xffffffffu, e < size && val[e] > avg);
+        G += __popc(gt[c]);
+    }
+    const int Lc = size - G;
+    unsigned gL[NC], lU[NC];  // > avg below Lc, <= avg from Lc on
+    int m = 0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const int b0 = c * 32;
+        const unsigned lo = Lc >= b0 + 32 ? 0xffffffffu : (Lc <= b0 ? 0u : (1u << (Lc - b0)) - 1u);
+        const unsigned in = size >= b0 + 32 ? 0xffffffffu : (size <= b0 ? 0u : (1u << (size - b0)) - 1u);
+        gL[c] = gt[c] & lo;
+        lU[c] = ~gt[c] & in & ~lo;
+        m += __popc(gL[c]);
+    }
+    if (m == 0) return Lc;
+    // the swaps pair positions, so each position takes its partner's entry
+    const unsigned below = (1u << lane) - 1u;
+    int src[NC];
+    int rg = 0, ru = 0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        src[c] = -1;
+        if ((gL[c] >> lane) & 1u) src[c] = nth_bit_of<NC>(lU, m - 1 - (rg + __popc(gL[c] & below)));
+        else if ((lU[c] >> lane) & 1u) src[c] = nth_bit_of<NC>(gL, m - 1 - (ru + __popc(lU[c] & below)));
+        rg += __popc(gL[c]);
+        ru += __popc(lU[c]);
+    }
+    double x[NC];
+    uint16_t q[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+        if (src[c] >= 0) { x[c] = val[src[c]]; q[c] = pl[src[c]]; }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+        if (src[c] >= 0) { val[c * 32 + lane] = x[c]; pl[c * 32 + lane] = q[c]; }
+    __syncwarp();
+    return Lc;
+}
+// qpart_ef_vals by a warp: the threshold loop (avg += 1 until ef_min entries
+// qualify, the passes that cannot move an entry counted by bump_until) with
+// warp_qpart_b_vals as the pass.  A list holding a NaN keeps the serial loop
+// (lane 0), whose every pass runs; the values never change, only their order.
+template <int NC>
+__device__ __noinline__ int warp_qpart_ef_vals(uint16_t* pl, double* val, int size, double avg, int ef_min,
+                                                   int lane) {
+    if (size < ef_min) return size;
+    bool nan = false;
+    for (int e = lane; e < size; e += 32) nan |= (val[e] != val[e]);
+    if (__any_sync(0xffffffffu, nan)) {
+        int p = 0;
+        if (lane == 0) p = qpart_ef_vals(pl, val, size, avg, ef_min);
+        __syncwarp();
+        return __shfl_sync(0xffffffffu, p, 0);
+    }
+    constexpr int kLimit = 1 << 20;
+    for (int bump = 0; bump < kLimit;) {
+        const int p = warp_qpart_b_vals<NC>(pl, val, size, avg, lane);
+        if (p >= ef_min) return p;
+        double g = INFINITY;
+        for (int e = p + lane; e < size; e += 32) g = fmin(g, val[e]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) g = fmin(g, __shfl_xor_sync(0xffffffffu, g, o));
+        avg += 1;
+        ++bump;
+        bump_until(avg, bump, g, kLimit);
+    }
+    return size;
+}
+
 /* ------------------------------------------------------------------ */
 /* Ax=b of an irregular comb                                            */
 /* ------------------------------------------------------------------ */

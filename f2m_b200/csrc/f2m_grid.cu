@@ -15,8 +15,9 @@
 // k EF hops of its own nodes (its halo, in shared memory) can run k steps
 // alone: step t recomputes the nodes within k-t hops, and after k steps its
 // own nodes hold exactly the values k global steps would give (every node's
-// update is the same function of the same inputs).  One grid barrier then
-// covers k steps instead of one.  k is the largest depth whose halo and EF
+// update is the same function of the same inputs).  A block then waits only
+// for the CTAs it shares halo nodes with (their published block counts),
+// instead of a grid barrier per step.  k is the largest depth whose halo and EF
 // entries fit every CTA's shared memory (at most the block depth, 4 by
 // default); k = 0 falls back to one barrier per step.
 #include <cuda_runtime.h>
@@ -34,6 +35,7 @@ namespace f2m {
 constexpr int kGT = 1024;              // threads per CTA (one CTA per SM: fewer barrier arrivals)
 constexpr int kMaxBlk = 16;            // most Jacobi steps between two grid barriers
 constexpr int kMaxNl = 2048;           // most nodes in a CTA's halo
+constexpr int kHaloPf = 4;             // EF entries loaded ahead in the halo build
 constexpr unsigned long long kHEmpty = ~0ull;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -53,6 +55,9 @@ __device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned* p, unsigned x
 }
 __device__ __forceinline__ void red_add_release_u32(unsigned* p, unsigned x) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(x) : "memory");
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned x) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(x) : "memory");
 }
 
 // Potentials written by other SMs are read through L2 (ld.global.cg): the
@@ -110,42 +115,6 @@ __device__ __forceinline__ double grad_half(int n, const double* Dp, const uint3
     return (-(a1 + a2) / 2) * 0.5;
 }
 
-// qpart_ptr_EF on a node's list copied to shared memory: `pl` holds the list
-// order and `val` the reduced cost of each position.  The loop is qpart_ef's
-// (the Hoare scans, the swaps, which move both arrays, and the threshold
-// sequence), so the final order and count are the same; only the values are
-// read from shared memory instead of three dependent global loads each.
-__device__ int qpart_b_vals(uint16_t* pl, double* val, int size, double avg) {
-    int low = 0, high = size - 1, i = low, j = high;
-    for (int pass = 0; i < j && pass <= size; ++pass) {
-        while (i <= high && val[i] <= avg) i++;
-        while (j >= low && val[j] > avg) j--;
-        if (i < j) {
-            const uint16_t t = pl[i]; pl[i] = pl[j]; pl[j] = t;
-            const double u = val[i]; val[i] = val[j]; val[j] = u;
-        }
-    }
-    return j + 1;
-}
-__device__ int qpart_ef_vals(uint16_t* pl, double* val, int size, double avg, int ef_min) {
-    if (size < ef_min) return size;
-    constexpr int kLimit = 1 << 20;
-    for (int bump = 0; bump < kLimit;) {
-        const int p = qpart_b_vals(pl, val, size, avg);
-        if (p >= ef_min) return p;
-        double g = INFINITY;
-        bool nan = false;
-        for (int k = 0; k < size; ++k) {
-            nan |= (val[k] != val[k]);
-            if (k >= p) g = fmin(g, val[k]);
-        }
-        avg += 1;
-        ++bump;
-        if (nan) continue;
-        bump_until(avg, bump, g, kLimit);
-    }
-    return size;
-}
 constexpr int kPartCap = 128;  // longest list partitioned in shared memory by a warp
 
 // Open-addressing table node -> local index in shared memory (the halo
@@ -174,6 +143,51 @@ __device__ __forceinline__ bool h_insert(unsigned long long* ht, unsigned mask, 
         if ((cur >> 32) == (unsigned)key) return true;
     }
     return false;
+}
+// h_insert for a whole warp (every lane calls it; key -1: nothing to
+// insert): each lane claims its key's slot, then one counter update per
+// warp numbers the keys claimed.  Returns false in a lane whose table probe
+// found no room.
+__device__ __forceinline__ bool h_insert_warp(unsigned long long* ht, unsigned mask, int key, int* count,
+                                              int* map, int nl, int lane) {
+    int slot = -1;
+    bool ok = true;
+    if (key >= 0) {
+        volatile unsigned long long* vt = ht;
+        const unsigned long long tag = (unsigned long long)(unsigned)key << 32;
+        unsigned h = hslot(key, mask);
+        ok = false;
+        for (unsigned p = 0; p <= mask; ++p, h = (h + 1) & mask) {
+            unsigned long long cur = vt[h];
+            if (cur == kHEmpty) {
+                cur = atomicCAS(ht + h, kHEmpty, tag | 0xffffffffull);
+                if (cur == kHEmpty) { slot = (int)h; ok = true; break; }
+            }
+            if ((cur >> 32) == (unsigned)key) { ok = true; break; }
+        }
+    }
+    const unsigned fm = __ballot_sync(0xffffffffu, slot >= 0);
+    if (fm) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(count, __popc(fm));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (slot >= 0) {
+            const int idx = base + __popc(fm & ((1u << lane) - 1u));
+            if (idx < nl) map[idx] = key;
+            atomicExch(ht + slot, ((unsigned long long)(unsigned)key << 32) | (unsigned)idx);
+        }
+    }
+    return ok;
+}
+// largest j in [0, n) with a[j] <= x (a ascending, a[0] <= x)
+__device__ __forceinline__ int upper_idx(const int* a, int n, int x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a[mid] <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 __device__ __forceinline__ int h_find(const unsigned long long* ht, unsigned mask, int key) {
     unsigned h = hslot(key, mask);
@@ -233,6 +247,10 @@ struct GridSolver {
     int* swarp;
     unsigned long long* sbcv;  // shared broadcast slot of the grid reductions
     int* sflag;                // shared: barrier error flag of this CTA
+    int* snb;                  // shared: neighbour CTAs of the halo blocks
+    int* snbn;                 // shared: their count
+    unsigned* swm;             // shared: mask of the CTAs whose nodes the halo reads
+    unsigned pcount = 0;       // halo blocks this CTA has completed
     Halo L;
     int phase = 0;
     long long iters = 0, wslots = 0;
@@ -273,6 +291,41 @@ struct GridSolver {
         __syncthreads();
         dead = *sflag != 0;
         return !dead;
+    }
+    // Neighbour waits of the halo blocks.  A block of CTA c reads the
+    // potentials of the nodes within K hops of its own (other CTAs' nodes)
+    // from one buffer and writes its own nodes to the other, so before block
+    // j it needs (a) block j-1 of every CTA whose nodes it reads (their
+    // values) and (b) block j-1 of every CTA that reads its nodes (those
+    // finished reading the buffer that block j overwrites).  Each CTA
+    // publishes its completed block count (a release store by thread 0 after
+    // a CTA barrier, as the grid barrier's arrival); warp 0 waits, one
+    // neighbour per lane, with acquire loads bounded like the grid barrier.  CTAs that share no halo node do not
+    // wait on each other.
+    __device__ bool wait_neighbours() {
+        if (threadIdx.x < 32) {
+            int bad = 0;
+            if (threadIdx.x == 0) bad = ld_acquire_i32(G.err);
+            bad = __shfl_sync(0xffffffffu, bad, 0);
+            const int n = *snbn;
+            for (int j = threadIdx.x; j < n && !bad; j += 32) {
+                const unsigned* f = G.prog + snb[j];
+                for (long long spins = 1; (int)(ld_acquire_u32(f) - pcount) < 0; ++spins) {
+                    if ((spins & 63) == 0 && ld_acquire_i32(G.err) != 0) { bad = 1; break; }
+                    if (spins > P.spin_limit) { atomicExch(G.err, 1); bad = 1; break; }
+                }
+            }
+            bad = __any_sync(0xffffffffu, bad);
+            if (threadIdx.x == 0) *sflag = bad;
+        }
+        __syncthreads();
+        dead = *sflag != 0;
+        return !dead;
+    }
+    __device__ void publish_block() {
+        __syncthreads();  // every own potential of the block is written
+        if (threadIdx.x == 0) st_release_u32(G.prog + blockIdx.x, pcount + 1);  // releases the CTA's writes
+        ++pcount;
     }
     // Deterministic grid reductions through per-CTA partials (double-buffered).
     // After the barrier one warp per CTA reads the partials (lane-strided, then
@@ -393,7 +446,8 @@ struct GridSolver {
         L.built = true;
         L.K = 0;
         if (L.nl == 0) return;
-        sync();  // every CTA's efc and arena lists are complete
+        for (int w = threadIdx.x; w < kGridNbWords; w += kGT) G.nbm[(size_t)blockIdx.x * kGridNbWords + w] = 0;
+        sync();  // every CTA's efc and arena lists are complete (and the reader rows clear)
         if (dead) return;
         unsigned long long* ht = reinterpret_cast<unsigned long long*>(L.h);
         const unsigned mask = 2u * (unsigned)L.nl - 1u;
@@ -412,13 +466,43 @@ struct GridSolver {
             __syncthreads();
             for (int d = 1; d <= L.kmax && depth == d - 1; ++d) {
                 const int f0 = d == 1 ? 0 : L.lend[d - 2], f1 = L.lend[d - 1];
-                for (int i = f0 + threadIdx.x; i < f1; i += kGT) {
-                    const int u = L.map[i];
-                    const int n = __ldcg(G.efc + u);
-                    const int64_t go = I.row[u] - row0;
-                    for (int k = 0; k < n; ++k)
-                        if (!h_insert(ht, mask, (int)(__ldcg(G.gW + go + k) & 0x7fffffffu), L.cnt, L.map, L.nl))
-                            L.cnt[1] = 1;
+                // the frontier's EF entries, flattened (a thread per entry, so
+                // a long list does not hold up its level): prefix of the list
+                // lengths in pre, first slot of each list in gof (the entry
+                // arrays are free while the levels are built)
+                const int F = f1 - f0;
+                int* pre = reinterpret_cast<int*>(L.W);
+                long long* gof = reinterpret_cast<long long*>(L.D);
+                int carry = 0;
+                for (int r = 0; r < F; r += kGT) {
+                    const int j = r + threadIdx.x;
+                    int n = 0;
+                    if (j < F) {
+                        const int u = L.map[f0 + j];
+                        n = __ldcg(G.efc + u);
+                        gof[j] = I.row[u] - row0;
+                    }
+                    int tot;
+                    const int ex = block_excl_scan<kGT>(n, swarp, &tot);
+                    if (j < F) pre[j] = carry + ex;
+                    carry += tot;
+                }
+                __syncthreads();
+                const int lane = threadIdx.x & 31;
+                for (int e0 = 0; e0 < carry; e0 += kHaloPf * kGT) {  // same trip count in a warp
+                    int key[kHaloPf];
+#pragma unroll
+                    for (int c = 0; c < kHaloPf; ++c) {  // the chunk's loads in flight together
+                        const int e = e0 + c * kGT + threadIdx.x;
+                        key[c] = -1;
+                        if (e < carry) {
+                            const int j = upper_idx(pre, F, e);
+                            key[c] = (int)(__ldcg(G.gW + gof[j] + (e - pre[j])) & 0x7fffffffu);
+                        }
+                    }
+#pragma unroll
+                    for (int c = 0; c < kHaloPf; ++c)
+                        if (!h_insert_warp(ht, mask, key[c], L.cnt, L.map, L.nl, lane)) L.cnt[1] = 1;
                 }
                 __syncthreads();
                 const int c = L.cnt[0], full = L.cnt[1];
@@ -438,12 +522,15 @@ struct GridSolver {
             const int nc = L.lend[depth - 1];  // <= nl
             L.hist[threadIdx.x] = 0;
             __syncthreads();
+            long long* order = reinterpret_cast<long long*>(L.D);  // (length, node) in the new order, staged
+            int* len = reinterpret_cast<int*>(L.W);                  // list lengths, staged
             for (int i = threadIdx.x; i < nc; i += kGT) {  // bucket and rank, staged in nn
                 const int n = __ldcg(G.efc + L.map[i]);
                 int lvl = 0;
                 while (i >= L.lend[lvl]) ++lvl;
                 const int key = lvl * 64 + 63 - min(n, 63);
                 L.nn[i] = (key << 16) | atomicAdd(L.hist + key, 1);
+                len[i] = n;
             }
             __syncthreads();
             {
@@ -453,19 +540,18 @@ struct GridSolver {
                 L.hist[threadIdx.x] = ex;
             }
             __syncthreads();
-            int* order = reinterpret_cast<int*>(L.D);  // the new order, staged in the entry array
             for (int i = threadIdx.x; i < nc; i += kGT) {
                 const int kr = L.nn[i];
-                order[L.hist[kr >> 16] + (kr & 0xffff)] = L.map[i];
+                order[L.hist[kr >> 16] + (kr & 0xffff)] = ((long long)len[i] << 32) | (unsigned)L.map[i];
             }
             __syncthreads();
             for (int i = threadIdx.x; i < nc; i += kGT) {
-                const int u = order[i];
+                const long long o = order[i];
+                const int u = (int)(unsigned)o;
                 L.map[i] = u;
+                L.nn[i] = (int)(o >> 32);
                 h_set(ht, mask, u, i);
             }
-            __syncthreads();
-            for (int i = threadIdx.x; i < nc; i += kGT) L.nn[i] = __ldcg(G.efc + L.map[i]);
             __syncthreads();
             // slice widths (warp-wide max) and their prefix
             const int ns = (nc + 31) / 32;
@@ -489,18 +575,39 @@ struct GridSolver {
         if (threadIdx.x == 0) L.cnt[1] = 0;
         __syncthreads();
         if (kc >= 1) {
+            // a thread per SELL position (padding positions skip): slice s
+            // holds positions [sb[s], sb[s+1]), entry k of its node i at
+            // sb[s] + 32 k + i % 32
             const int nc = L.lend[kc - 1];
-            for (int i = threadIdx.x; i < nc; i += kGT) {
-                const int u = L.map[i];
-                const int n = L.nn[i];
-                const int64_t go = I.row[u] - row0;
-                const int base = L.sb[i >> 5] + (i & 31);
-                for (int k = 0; k < n; ++k) {
-                    const uint32_t w = __ldcg(G.gW + go + k);
-                    const int li = h_find(ht, mask, (int)(w & 0x7fffffffu));
+            const int ns = (nc + 31) / 32;
+            const int np = L.sb[ns];
+            for (int p0 = 0; p0 < np; p0 += kHaloPf * kGT) {
+                uint32_t w[kHaloPf];
+                double dd[kHaloPf];
+                int pos[kHaloPf];
+#pragma unroll
+                for (int c = 0; c < kHaloPf; ++c) {  // the chunk's loads in flight together
+                    const int p = p0 + c * kGT + threadIdx.x;
+                    pos[c] = -1;
+                    if (p < np) {
+                        const int sl = upper_idx(L.sb, ns, p);
+                        const int r = p - L.sb[sl];
+                        const int i = sl * 32 + (r & 31), k = r >> 5;
+                        if (i < nc && k < L.nn[i]) {
+                            const int64_t go = I.row[L.map[i]] - row0 + k;
+                            w[c] = __ldcg(G.gW + go);
+                            dd[c] = __ldcg(G.gD + go);
+                            pos[c] = p;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < kHaloPf; ++c) {
+                    if (pos[c] < 0) continue;
+                    const int li = h_find(ht, mask, (int)(w[c] & 0x7fffffffu));
                     if (li < 0 || li >= L.lend[kc]) L.cnt[1] = 1;  // cannot happen: all within kc hops
-                    L.D[base + 32 * k] = __ldcg(G.gD + go + k);
-                    L.W[base + 32 * k] = (uint32_t)(li < 0 ? 0 : li) | (w & 0x80000000u);
+                    L.D[pos[c]] = dd[c];
+                    L.W[pos[c]] = (uint32_t)(li < 0 ? 0 : li) | (w[c] & 0x80000000u);
                 }
             }
         }
@@ -510,10 +617,38 @@ struct GridSolver {
         for (int i = threadIdx.x; i < nown(); i += kGT) L.own_slots += G.efc[node(i)];
         L.K = (int)(-gmax_ll(-(long long)kc));
         __syncthreads();
+        // neighbour CTAs of the blocks: the owners of the nodes the blocks
+        // read (levels 1..K) and the CTAs whose blocks read this CTA's nodes
+        if (L.K > 0) {
+            for (int w = threadIdx.x; w < kGridNbWords; w += kGT) swm[w] = 0;
+            __syncthreads();
+            for (int i = L.lend[0] + threadIdx.x; i < L.lend[L.K]; i += kGT) {
+                const int c = __ldcg(G.owner + L.map[i]);
+                if (c != (int)blockIdx.x) atomicOr(swm + (c >> 5), 1u << (c & 31));
+            }
+            __syncthreads();
+            for (int w = threadIdx.x; w < kGridNbWords; w += kGT)
+                for (unsigned m = swm[w]; m; m &= m - 1) {
+                    const int c = w * 32 + __ffs(m) - 1;
+                    atomicOr(G.nbm + (size_t)c * kGridNbWords + (blockIdx.x >> 5), 1u << (blockIdx.x & 31));
+                }
+            sync();
+            if (threadIdx.x == 0) {
+                int cnt = 0;
+                for (int w = 0; w < kGridNbWords; ++w) {
+                    unsigned m = swm[w] | __ldcg(G.nbm + (size_t)blockIdx.x * kGridNbWords + w);
+                    if (w == (int)(blockIdx.x >> 5)) m &= ~(1u << (blockIdx.x & 31));
+                    for (; m; m &= m - 1) snb[cnt++] = w * 32 + __ffs(m) - 1;
+                }
+                *snbn = cnt;
+            }
+            __syncthreads();
+        }
     }
 
-    // n unmasked Jacobi steps: blocks of K halo steps with one grid barrier
-    // each, or single global steps when no halo fits
+    // n unmasked Jacobi steps: blocks of K halo steps, each after a wait on
+    // the neighbour CTAs only, and one grid barrier at the end; or single
+    // global steps (a grid barrier each) when no halo fits
     __device__ void steps(int n) {
         if (!L.built) build_halo();
         if (L.K == 0) {
@@ -524,8 +659,11 @@ struct GridSolver {
         double* Bn = L.h + L.nl;
         for (int done = 0; done < n && !dead;) {
             const int k = min(L.K, n - done);
+            if (!wait_neighbours()) break;
             const L2Ptr H = hc();
-            for (int i = threadIdx.x; i < L.lend[k]; i += kGT) A[i] = H[L.map[i]];
+            // after the first block the own nodes ([0, lend[0])) already hold
+            // this CTA's last values in A
+            for (int i = (done == 0 ? 0 : L.lend[0]) + threadIdx.x; i < L.lend[k]; i += kGT) A[i] = H[L.map[i]];
             __syncthreads();
             for (int t = 1; t <= k; ++t) {
                 const int m = L.lend[k - t];  // nodes within k-t hops
@@ -543,9 +681,10 @@ struct GridSolver {
             wslots += (long long)k * L.own_slots;
             iters += k;
             done += k;
-            sync();
+            publish_block();
             swap_h();
         }
+        sync();  // every CTA's last block is written before grid-wide reads of H
     }
 
     // update_EF's partitions of the own nodes' lists (cuda_partition_v2 with
@@ -553,8 +692,8 @@ struct GridSolver {
     // when glob): warp w takes the own nodes w, w+32, ...; a list of up to
     // kPartCap entries is copied with its reduced costs into the warp's
     // shared scratch in one parallel round of loads and partitioned there by
-    // one lane (the halo region is free here: it is rebuilt after every
-    // update_EF); one lane runs the global-memory partition for a longer
+    // the whole warp (warp_qpart_ef_vals; the halo region is free here: it is
+    // rebuilt after every update_EF); one lane runs the global-memory partition for a longer
     // list.  Without the scratch (no halo), a thread per node partitions in
     // global memory.
     __device__ void partition_own(bool glob, double thr) {
@@ -591,25 +730,34 @@ struct GridSolver {
             uint16_t* list = I.perm + r0;
             int p = 0;
             if (d <= kPartCap) {
+                // pslot holds the slots in list order, so a reduced cost is two
+                // dependent loads (the slot, then the neighbour's potential)
                 const double hv = H[v];
-                for (int k = lane; k < d; k += 32) {
-                    const uint16_t q = list[k];
-                    pl[k] = q;
-                    val[k] = red_d(I.slot[r0 + q], v, H, hv);
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    double avg = thr;
-                    if (glob) {
-                        avg = val[0];
-                        for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, val[k]);
+                uint16_t q0[kPartCap / 32];
+#pragma unroll
+                for (int c = 0; c < kPartCap / 32; ++c) {
+                    const int k = c * 32 + lane;
+                    if (k < d) {
+                        q0[c] = list[k];
+                        pl[k] = q0[c];
+                        val[k] = red_d(I.pslot[r0 + k], v, H, hv);
                     }
-                    p = qpart_ef_vals(pl, val, d, avg, P.ef_min);
                 }
                 __syncwarp();
-                for (int k = lane; k < d; k += 32) {
-                    list[k] = pl[k];
-                    I.pslot[r0 + k] = I.slot[r0 + pl[k]];
+                double avg = thr;
+                if (glob) {
+                    avg = val[0];
+                    for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, val[k]);
+                }
+                p = warp_qpart_ef_vals<kPartCap / 32>(pl, val, d, avg, P.ef_min, lane);
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < kPartCap / 32; ++c) {  // only the positions the swaps changed
+                    const int k = c * 32 + lane;
+                    if (k < d && pl[k] != q0[c]) {
+                        list[k] = pl[k];
+                        I.pslot[r0 + k] = I.slot[r0 + pl[k]];
+                    }
                 }
                 __syncwarp();
             } else if (lane == 0) {
@@ -632,10 +780,11 @@ struct GridSolver {
         checks++;
         return grad_max();
     }
-    __device__ void block_ef(int N) {
-        // cuda_block_EF: N steps, or check_every when the gradient at entry is
-        // already below error_B (the count check breaks there)
-        const double MA = grad_max();
+    // cuda_block_EF: N steps, or check_every when the gradient at entry is
+    // already below error_B (the count check breaks there).  Every call
+    // follows a check_OPT whose max |grad| was taken over the same
+    // potentials and active sets, so that value is the entry gradient MA.
+    __device__ void block_ef(int N, double MA) {
         steps(MA < P.error_B ? min(N, P.check_every) : N);
     }
     __device__ void block_glob() {
@@ -656,7 +805,7 @@ struct GridSolver {
         double M = check_opt();
         int factor = P.factor0;
         for (int go = 1; go <= P.max_rounds && !dead; ++go) {
-            block_ef(factor);
+            block_ef(factor, M);
             M = check_opt();
             if (factor < P.factor_cap) factor += P.factor_step;
             if (M < P.error_B) break;
@@ -667,7 +816,7 @@ struct GridSolver {
     __device__ double run_fix() {
         double M = check_opt();
         for (int go = 1; go <= P.fix_rounds && !dead; ++go) {
-            block_ef(P.fix_factor);
+            block_ef(P.fix_factor, M);
             M = check_opt();
             if (M < P.error_B) break;
             if (iters > P.max_iters) { capped = true; break; }
@@ -867,6 +1016,9 @@ __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, Gri
     __shared__ int scnt[2];
     __shared__ int ssb[kMaxNl / 32 + 1];
     __shared__ int shist[kGT];
+    __shared__ int snb[kGridMaxCtas];
+    __shared__ int snbn[1];
+    __shared__ unsigned swm[kGridNbWords];
     const Inst I = make_inst(B, b);
     const int V = I.V;
     const int o0 = (int)(((long long)V * blockIdx.x) / gridDim.x);
@@ -880,7 +1032,9 @@ __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, Gri
     off += (size_t)cap * 8;
     uint32_t* eW = reinterpret_cast<uint32_t*>(smem_raw + off);
     off += ((size_t)cap * 4 + 15) / 16 * 16;
-    GridSolver S{B, P, G, I, b, o0, o1, I.row[0], G.Ha, G.Hb, eD, eW, cap, sefo, sred, sredl, swarp, sbc, sflag};
+    GridSolver S{B, P, G, I, b, o0, o1, I.row[0], G.Ha, G.Hb, eD, eW, cap, sefo, sred, sredl, swarp, sbc, sflag,
+                 snb, snbn, swm};
+    if (threadIdx.x == 0) snbn[0] = 0;
     S.L.h = reinterpret_cast<double*>(smem_raw + off);
     off += (size_t)nl * 16;
     S.L.map = reinterpret_cast<int*>(smem_raw + off);
@@ -898,6 +1052,7 @@ __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, Gri
     S.L.ne = ne;
     S.L.kmax = min(kmax, kMaxBlk);
     double M;
+    for (int i = threadIdx.x; i < nv; i += kGT) G.owner[S.node(i)] = (int32_t)blockIdx.x;
     // the own nodes' slots in list order (the host paths upload slot and perm)
     for (int i = threadIdx.x; i < nv; i += kGT) {
         const int v = S.node(i);
@@ -998,6 +1153,7 @@ cudaError_t launch_solve_grid(const Batch& B, const DevParams& P, const GridStat
     if ((e = cudaMemsetAsync(G.bar, 0, 2 * sizeof(unsigned), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(G.axb_used, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(G.err, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(G.prog, 0, kGridMaxCtas * sizeof(unsigned), s)) != cudaSuccess) return e;
     Batch Bc = B;
     DevParams Pc = P;
     GridState Gc = G;

@@ -146,12 +146,16 @@ struct GridState {
     double* part;           // [2*grid] partial reductions
     long long* partl;       // [2*grid]
     int32_t* own;           // [V] nodes in ownership order (CTA c owns a contiguous run)
+    int32_t* owner;         // [V] CTA owning each node
+    unsigned* prog;         // [kGridMaxCtas] halo blocks each CTA has completed (neighbour waits)
+    unsigned* nbm;          // [kGridMaxCtas * kGridNbWords] bit d of row c: CTA d reads c's nodes
     unsigned long long* okey;   // [V] ownership sort keys (Morton code << 32 | node)
     unsigned long long* okey2;  // [V]
     void* otmp;             // radix-sort scratch
     size_t otmp_bytes;
 };
 constexpr int kGridMaxCtas = 2 * 160;
+constexpr int kGridNbWords = kGridMaxCtas / 32;  // words of one neighbour-mask row
 
 // Host-side launchers (f2m_kernels.cu, f2m_grid.cu).
 cudaError_t launch_solve_grid(const Batch& B, const DevParams& P, const GridState& G, int b, int V,
@@ -193,6 +197,8 @@ cudaError_t launch_edge_order(const Batch& B, int b, int V, int64_t S, const Edg
 // FP64 pipe throughput probe (f2m_probe.cu): kind 0 DADD chains, kind 1 DSETP.
 cudaError_t launch_fp64_probe(int kind, int blocks, int iters, double* out, cudaStream_t s);
 double fp64_probe_ops(int kind, int blocks, int iters);
+cudaError_t launch_partition_check(int n_cases, unsigned long long seed, unsigned long long* bad,
+                                   cudaStream_t s);
 cudaError_t launch_prep(const Batch& B, cudaStream_t s, int64_t* launches);
 // Ax=b of the irregular combs and the primal of every instance the solver
 // left with status kNeedsAxb (one CTA per instance of the batch).

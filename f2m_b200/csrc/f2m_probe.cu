@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "f2m_device.cuh"
 #include "f2m_internal.h"
 
 namespace f2m {
@@ -61,6 +62,61 @@ double fp64_probe_ops(int kind, int blocks, int iters) {
 cudaError_t launch_fp64_probe(int kind, int blocks, int iters, double* out, cudaStream_t s) {
     if (kind == 0) k_fp64_rate<0><<<blocks, kProbeThreads, 0, s>>>(out, iters, 0.37);
     else k_fp64_rate<1><<<blocks, kProbeThreads, 0, s>>>(out, iters, 0.37);
+    return cudaGetLastError();
+}
+
+// Self-check of the warp-cooperative partition (diagnostics): every warp
+// draws seeded lists (sizes 0-128, values from a few levels so that ties and
+// runs are common, thresholds that force the raise-by-one loop, an
+// occasional NaN), partitions one copy with the serial loop (qpart_ef_vals,
+// lane 0) and one with warp_qpart_ef_vals, and counts the lists whose final
+// order or count differ.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+constexpr int kPcWarps = 8;
+constexpr int kPcCap = 128;
+__global__ void __launch_bounds__(32 * kPcWarps) k_partition_check(int n_cases, unsigned long long seed,
+                                                                    unsigned long long* bad) {
+    __shared__ double sv[kPcWarps][2][kPcCap];
+    __shared__ uint16_t sp[kPcWarps][2][kPcCap];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cs = blockIdx.x * kPcWarps + w;
+    if (cs >= n_cases) return;
+    const unsigned long long h = mix64(seed ^ mix64((unsigned long long)cs));
+    const int kind = (int)(h % 5);
+    const int size = (kind == 4) ? (int)((h >> 8) % 6) : (int)((h >> 8) % (kPcCap + 1));
+    const int levels = 1 + (int)((h >> 20) % 40);
+    const bool nan = ((h >> 32) % 50) == 0;
+    for (int e = lane; e < kPcCap; e += 32) {
+        const unsigned long long r = mix64(h + (unsigned long long)e);
+        double x = (kind == 0) ? (double)(r >> 11) * 0x1.0p-53 * 4.0 - 1.0
+                               : (double)(r % (unsigned long long)levels) * 0.5 - 2.0;
+        if (nan && e == (int)((h >> 40) % (unsigned long long)(size > 0 ? size : 1))) x = NAN;
+        sv[w][0][e] = sv[w][1][e] = x;
+        sp[w][0][e] = sp[w][1][e] = (uint16_t)e;
+    }
+    __syncwarp();
+    const double avg = (kind == 1) ? -3.0 - (double)((h >> 48) % 7) : (double)((int)((h >> 48) % 9) - 4) * 0.25;
+    const int ef_min = 1 + (int)((h >> 56) % 6);
+    int p0 = 0;
+    if (lane == 0) p0 = qpart_ef_vals(sp[w][0], sv[w][0], size, avg, ef_min);
+    __syncwarp();
+    p0 = __shfl_sync(0xffffffffu, p0, 0);
+    const int p1 = warp_qpart_ef_vals<kPcCap / 32>(sp[w][1], sv[w][1], size, avg, ef_min, lane);
+    __syncwarp();
+    bool diff = p0 != p1;
+    for (int e = lane; e < size; e += 32) diff |= sp[w][0][e] != sp[w][1][e];
+    if (__any_sync(0xffffffffu, diff) && lane == 0) atomicAdd(bad, 1ull);
+}
+
+cudaError_t launch_partition_check(int n_cases, unsigned long long seed, unsigned long long* bad, cudaStream_t s) {
+    if (n_cases <= 0) return cudaSuccess;
+    const int blocks = (n_cases + kPcWarps - 1) / kPcWarps;
+    k_partition_check<<<blocks, 32 * kPcWarps, 0, s>>>(n_cases, seed, bad);
     return cudaGetLastError();
 }
 

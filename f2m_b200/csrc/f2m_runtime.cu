@@ -213,6 +213,9 @@ void carve_grid(Arena& A, GridState& G, int64_t n, int64_t S) {
     G.part = A.take<double>(2 * kGridMaxCtas);
     G.partl = A.take<long long>(2 * kGridMaxCtas);
     G.own = A.take<int32_t>(n);
+    G.owner = A.take<int32_t>(n);
+    G.prog = A.take<unsigned>(kGridMaxCtas);
+    G.nbm = A.take<unsigned>((int64_t)kGridMaxCtas * kGridNbWords);
     G.okey = A.take<unsigned long long>(n);
     G.okey2 = A.take<unsigned long long>(n);
     G.otmp_bytes = grid_order_temp_bytes(n);
@@ -1327,6 +1330,22 @@ f2m_status f2m_fp64_rate(f2m_ctx* ctx, int32_t kind, int32_t repeats, double* la
     }
     ctx->timed = false;  // the phase events now hold the probe's times
     *lane_ops_per_s = best;
+    return F2M_OK;
+}
+
+f2m_status f2m_partition_selfcheck(f2m_ctx* ctx, int32_t n_cases, uint64_t seed, int64_t* mismatches) {
+    if (!ctx || !mismatches || n_cases < 0)
+        return fail(ctx, F2M_ERR_INPUT, "f2m_partition_selfcheck: n_cases >= 0 and an output pointer");
+    F2M_CUDA(cudaSetDevice(ctx->device));
+    F2M_CUDA(ensure_device(ctx, 4096));
+    unsigned long long* bad = reinterpret_cast<unsigned long long*>(ctx->dev);
+    F2M_CUDA(cudaMemsetAsync(bad, 0, sizeof(*bad), ctx->stream));
+    F2M_CUDA(launch_partition_check(n_cases, seed, bad, ctx->stream));
+    ctx->launches++;
+    unsigned long long h = 0;
+    F2M_CUDA(cudaMemcpyAsync(&h, bad, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    *mismatches = (int64_t)h;
     return F2M_OK;
 }
 

@@ -143,6 +143,14 @@ f2m_status f2m_phase_times(f2m_ctx* ctx, float* ms, f2m_work* work);
  * launches (CUDA events) over every SM at full occupancy. */
 f2m_status f2m_fp64_rate(f2m_ctx* ctx, int32_t kind, int32_t repeats, double* lane_ops_per_s);
 
+/* Self-check of the warp-cooperative list partition (diagnostics; no
+ * reference counterpart): runs n_cases seeded lists (0-128 entries, many
+ * ties, thresholds that need the raise-by-one loop of qpart_ptr_EF,
+ * graph_cuda_partition.hpp:27-54) through the serial partition and the warp
+ * partition on the device and returns how many differ in order or count
+ * (0 when they agree). */
+f2m_status f2m_partition_selfcheck(f2m_ctx* ctx, int32_t n_cases, uint64_t seed, int64_t* mismatches);
+
 /* ------------------------------------------------------------------ */
 /* Single instance with full results (the F2M.h graph API).             */
 /* ------------------------------------------------------------------ */

@@ -456,3 +456,13 @@ def test_grid_barrier_wait_runs_out_and_the_context_recovers(ctx):
     finally:
         fresh.close()
     assert r.status == 0 and np.array_equal(r.F, r2.F) and r.lp == r2.lp
+
+
+def test_warp_partition_equals_the_serial_loop(ctx):
+    """The whole-GPU solver partitions a node's list with a whole warp
+    (qpart_ptr_EF, graph_cuda_partition.hpp:27-54, restated as a fixed
+    pairing of swaps ranked by ballots).  On the device, 200,000 seeded lists
+    (0-128 entries, ties, thresholds that need the raise-by-one loop, NaN)
+    must come out in the serial loop's order with its count."""
+    assert ctx.partition_selfcheck(200000, 7) == 0
+    assert ctx.partition_selfcheck(200000, 8) == 0
