@@ -340,31 +340,14 @@ __device__ inline int qpart_ef_vals(uint16_t* pl, double* val, int size, double 
 // the t-th entry <= avg of [Lc, size) (descending), for every t below the
 // number m of entries > avg in [0, Lc), and it returns Lc (a list of one
 // entry is returned as it is: the loop does not run).  Each lane ranks its
-// entries with ballots and moves the ones that swap, so the final order and
-// the count are the serial loop's.  Lists of at most 32 * NC entries in
-// shared memory; every lane of the warp calls it with the same arguments.
-__device__ __forceinline__ int nth_bit(unsigned m, int n) {  // position of the n-th (0-based) set bit
-    int pos = 0;
-#pragma unroll
-    for (int w = 16; w >= 1; w >>= 1) {
-        const int c = __popc(m & ((1u << w) - 1u));
-        if (n >= c) { n -= c; m >>= w; pos += w; }
-    }
-    return pos;
-}
+// entries with ballots, the two sides list their positions by rank in
+// `pos` (2 x 16 NC bytes: m <= size / 2), and the entries that swap take
+// their partner's, so the final order and the count are the serial loop's.
+// Lists of at most 32 * NC entries in shared memory; every lane of the warp
+// calls it with the same arguments.
 template <int NC>
-__device__ __forceinline__ int nth_bit_of(const unsigned (&m)[NC], int n) {
-    int r = -1;
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        const int pc = __popc(m[c]);
-        if (r < 0 && n < pc) r = c * 32 + nth_bit(m[c], n);
-        n -= pc;
-    }
-    return r;
-}
-template <int NC>
-__device__ __forceinline__ int warp_qpart_b_vals(uint16_t* pl, double* val, int size, double avg, int lane) {
+__device__ __forceinline__ int warp_qpart_b_vals(uint16_t* pl, double* val, uint8_t* pos, int size, double avg,
+                                                 int lane) {
     if (size <= 1) return size;
     unsigned gt[NC];
     int G = 0;
@@ -375,35 +358,42 @@ __device__ __forceinline__ int warp_qpart_b_vals(uint16_t* pl, double* val, int 
         G += __popc(gt[c]);
     }
     const int Lc = size - G;
-    unsigned gL[NC], lU[NC];  // > avg below Lc, <= avg from Lc on
-    int m = 0;
+    // > avg below Lc (ranked ascending into pos[0..m)), <= avg from Lc on
+    // (ranked ascending into pos[16 NC ..)); the t-th of the first swaps with
+    // the (m-1-t)-th of the second
+    uint8_t* gp = pos;
+    uint8_t* up = pos + 16 * NC;
+    const unsigned below = (1u << lane) - 1u;
+    int rg = 0, ru = 0;
+    int rank[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         const int b0 = c * 32;
         const unsigned lo = Lc >= b0 + 32 ? 0xffffffffu : (Lc <= b0 ? 0u : (1u << (Lc - b0)) - 1u);
         const unsigned in = size >= b0 + 32 ? 0xffffffffu : (size <= b0 ? 0u : (1u << (size - b0)) - 1u);
-        gL[c] = gt[c] & lo;
-        lU[c] = ~gt[c] & in & ~lo;
-        m += __popc(gL[c]);
+        const unsigned gL = gt[c] & lo, lU = ~gt[c] & in & ~lo;
+        rank[c] = -1;
+        if ((gL >> lane) & 1u) { rank[c] = rg + __popc(gL & below); gp[rank[c]] = (uint8_t)(b0 + lane); }
+        if ((lU >> lane) & 1u) { rank[c] = ru + __popc(lU & below); up[rank[c]] = (uint8_t)(b0 + lane); }
+        rg += __popc(gL);
+        ru += __popc(lU);
     }
+    const int m = rg;  // == ru
     if (m == 0) return Lc;
-    // the swaps pair positions, so each position takes its partner's entry
-    const unsigned below = (1u << lane) - 1u;
+    __syncwarp();
     int src[NC];
-    int rg = 0, ru = 0;
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        src[c] = -1;
-        if ((gL[c] >> lane) & 1u) src[c] = nth_bit_of<NC>(lU, m - 1 - (rg + __popc(gL[c] & below)));
-        else if ((lU[c] >> lane) & 1u) src[c] = nth_bit_of<NC>(gL, m - 1 - (ru + __popc(lU[c] & below)));
-        rg += __popc(gL[c]);
-        ru += __popc(lU[c]);
-    }
     double x[NC];
     uint16_t q[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
-        if (src[c] >= 0) { x[c] = val[src[c]]; q[c] = pl[src[c]]; }
+    for (int c = 0; c < NC; ++c) {
+        src[c] = -1;
+        if (rank[c] >= 0) {
+            const bool low = c * 32 + lane < Lc;
+            src[c] = low ? up[m - 1 - rank[c]] : gp[m - 1 - rank[c]];
+            x[c] = val[src[c]];
+            q[c] = pl[src[c]];
+        }
+    }
     __syncwarp();
 #pragma unroll
     for (int c = 0; c < NC; ++c)
@@ -416,8 +406,8 @@ __device__ __forceinline__ int warp_qpart_b_vals(uint16_t* pl, double* val, int 
 // warp_qpart_b_vals as the pass.  A list holding a NaN keeps the serial loop
 // (lane 0), whose every pass runs; the values never change, only their order.
 template <int NC>
-__device__ __noinline__ int warp_qpart_ef_vals(uint16_t* pl, double* val, int size, double avg, int ef_min,
-                                                   int lane) {
+__device__ __noinline__ int warp_qpart_ef_vals(uint16_t* pl, double* val, uint8_t* pos, int size, double avg,
+                                              int ef_min, int lane) {
     if (size < ef_min) return size;
     bool nan = false;
     for (int e = lane; e < size; e += 32) nan |= (val[e] != val[e]);
@@ -429,7 +419,7 @@ __device__ __noinline__ int warp_qpart_ef_vals(uint16_t* pl, double* val, int si
     }
     constexpr int kLimit = 1 << 20;
     for (int bump = 0; bump < kLimit;) {
-        const int p = warp_qpart_b_vals<NC>(pl, val, size, avg, lane);
+        const int p = warp_qpart_b_vals<NC>(pl, val, pos, size, avg, lane);
         if (p >= ef_min) return p;
         double g = INFINITY;
         for (int e = p + lane; e < size; e += 32) g = fmin(g, val[e]);

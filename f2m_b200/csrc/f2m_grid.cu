@@ -222,6 +222,7 @@ struct Halo {
     int* sb;               // shared [kMaxNl/32+1]: first entry of each 32-node slice
     int* hist;             // shared [kGT]: counting-sort buckets (level, list length)
     int nl = 0, ne = 0;
+    int nb = 0;            // own nodes [0, nb) are read by other CTAs' halos
     int kmax = 0;
     int K = 0;             // steps per block of the current active sets (same on every CTA)
     bool built = false;
@@ -298,8 +299,8 @@ struct GridSolver {
     // j it needs (a) block j-1 of every CTA whose nodes it reads (their
     // values) and (b) block j-1 of every CTA that reads its nodes (those
     // finished reading the buffer that block j overwrites).  Each CTA
-    // publishes its completed block count (a release store by thread 0 after
-    // a CTA barrier, as the grid barrier's arrival); warp 0 waits, one
+    // publishes its completed block count (a release store after a CTA
+    // barrier, as the grid barrier's arrival); warp 0 waits, one
     // neighbour per lane, with acquire loads bounded like the grid barrier.  CTAs that share no halo node do not
     // wait on each other.
     __device__ bool wait_neighbours() {
@@ -324,7 +325,9 @@ struct GridSolver {
     }
     __device__ void publish_block() {
         __syncthreads();  // every own potential of the block is written
-        if (threadIdx.x == 0) st_release_u32(G.prog + blockIdx.x, pcount + 1);  // releases the CTA's writes
+        // the last warp releases the CTA's writes (its store waits for them),
+        // so warp 0 can already poll the neighbours of the next block
+        if (threadIdx.x == kGT - 32) st_release_u32(G.prog + blockIdx.x, pcount + 1);
         ++pcount;
     }
     // Deterministic grid reductions through per-CTA partials (double-buffered).
@@ -447,7 +450,8 @@ struct GridSolver {
         L.K = 0;
         if (L.nl == 0) return;
         for (int w = threadIdx.x; w < kGridNbWords; w += kGT) G.nbm[(size_t)blockIdx.x * kGridNbWords + w] = 0;
-        sync();  // every CTA's efc and arena lists are complete (and the reader rows clear)
+        for (int i = threadIdx.x; i < nown(); i += kGT) G.rd[node(i)] = 0;
+        sync();  // every CTA's efc and arena lists are complete (the reader rows and marks clear)
         if (dead) return;
         unsigned long long* ht = reinterpret_cast<unsigned long long*>(L.h);
         const unsigned mask = 2u * (unsigned)L.nl - 1u;
@@ -513,11 +517,21 @@ struct GridSolver {
                 __syncthreads();
             }
         }
+        // Mark the nodes of levels 1..depth (other CTAs' nodes this CTA's
+        // blocks read); after a grid barrier every CTA knows which of its own
+        // nodes other CTAs read, and a block computes and publishes those
+        // first.
+        if (depth >= 1)
+            for (int i = L.lend[0] + threadIdx.x; i < L.lend[depth]; i += kGT) G.rd[L.map[i]] = 1;
+        sync();
+        if (dead) return;
         // The nodes of levels < depth (the ones a block may recompute) are
         // renumbered level by level in decreasing list length, so the
         // 32-node slices of the SELL layout carry little padding; a counting
-        // sort over (level, 63 - min(length, 63)) keeps the levels in order.
+        // sort over (group, 31 - min(length, 31)) keeps the groups in order:
+        // own nodes other CTAs read, the other own nodes, then level 1, 2, ...
         int kc = 0;
+        L.nb = 0;
         if (depth >= 1) {
             const int nc = L.lend[depth - 1];  // <= nl
             L.hist[threadIdx.x] = 0;
@@ -528,7 +542,8 @@ struct GridSolver {
                 const int n = __ldcg(G.efc + L.map[i]);
                 int lvl = 0;
                 while (i >= L.lend[lvl]) ++lvl;
-                const int key = lvl * 64 + 63 - min(n, 63);
+                const int grp = lvl == 0 ? (__ldcg(G.rd + L.map[i]) ? 0 : 1) : lvl + 1;
+                const int key = grp * 32 + 31 - min(n, 31);
                 L.nn[i] = (key << 16) | atomicAdd(L.hist + key, 1);
                 len[i] = n;
             }
@@ -540,6 +555,7 @@ struct GridSolver {
                 L.hist[threadIdx.x] = ex;
             }
             __syncthreads();
+            L.nb = L.hist[32];  // own nodes other CTAs read
             for (int i = threadIdx.x; i < nc; i += kGT) {
                 const int kr = L.nn[i];
                 order[L.hist[kr >> 16] + (kr & 0xffff)] = ((long long)len[i] << 32) | (unsigned)L.map[i];
@@ -667,23 +683,36 @@ struct GridSolver {
             __syncthreads();
             for (int t = 1; t <= k; ++t) {
                 const int m = L.lend[k - t];  // nodes within k-t hops
-                for (int i = threadIdx.x; i < m; i += kGT) {
-                    const int lo = L.sb[i >> 5] + (i & 31);
-                    const double h = A[i];
-                    Bn[i] = h + grad_half<32>(L.nn[i], L.D + lo, L.W + lo, A, h);
+                // the last step updates the own nodes (m = lend[0]): those
+                // other CTAs read are written to H and published first; the
+                // rest stay in shared memory (written to H once, after the
+                // last block)
+                const bool last = t == k;
+                for (int part = 0; part < (last ? 2 : 1); ++part) {
+                    const int i0 = (last && part == 1) ? L.nb : 0;
+                    const int i1 = (last && part == 0) ? L.nb : m;
+                    for (int i = i0 + threadIdx.x; i < i1; i += kGT) {
+                        const int lo = L.sb[i >> 5] + (i & 31);
+                        const double h = A[i];
+                        const double hn = h + grad_half<32>(L.nn[i], L.D + lo, L.W + lo, A, h);
+                        Bn[i] = hn;
+                        if (last && part == 0) Hn[L.map[i]] = hn;
+                    }
+                    if (last && part == 0) publish_block();
                 }
                 __syncthreads();
                 double* t2 = A;
                 A = Bn;
                 Bn = t2;
             }
-            for (int i = threadIdx.x; i < nown(); i += kGT) Hn[L.map[i]] = A[i];
             wslots += (long long)k * L.own_slots;
             iters += k;
             done += k;
-            publish_block();
             swap_h();
         }
+        // the own nodes no other CTA reads, into the current buffer
+        if (n > 0)
+            for (int i = L.nb + threadIdx.x; i < L.lend[0] && !dead; i += kGT) Hc[L.map[i]] = A[i];
         sync();  // every CTA's last block is written before grid-wide reads of H
     }
 
@@ -698,9 +727,12 @@ struct GridSolver {
     // global memory.
     __device__ void partition_own(bool glob, double thr) {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        const bool scratch = L.nl > 0 && (long long)L.ne * 12 >= 32LL * kPartCap * 10;
+        // per warp: kPartCap values (8 B), list entries (2 B) and rank positions (1 B)
+        const bool scratch = L.nl > 0 && (long long)L.ne * 12 >= 32LL * kPartCap * 11;
         double* val = L.D + wid * kPartCap;
         uint16_t* pl = reinterpret_cast<uint16_t*>(L.D + 32 * kPartCap) + wid * kPartCap;
+        uint8_t* pos = reinterpret_cast<uint8_t*>(reinterpret_cast<uint16_t*>(L.D + 32 * kPartCap) + 32 * kPartCap) +
+                       wid * kPartCap;
         const L2Ptr H = hc();
         if (!scratch) {  // no shared scratch: a thread per node, in global memory
             for (int i = threadIdx.x; i < nown(); i += kGT) {
@@ -749,7 +781,7 @@ struct GridSolver {
                     avg = val[0];
                     for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, val[k]);
                 }
-                p = warp_qpart_ef_vals<kPartCap / 32>(pl, val, d, avg, P.ef_min, lane);
+                p = warp_qpart_ef_vals<kPartCap / 32>(pl, val, pos, d, avg, P.ef_min, lane);
                 __syncwarp();
 #pragma unroll
                 for (int c = 0; c < kPartCap / 32; ++c) {  // only the positions the swaps changed

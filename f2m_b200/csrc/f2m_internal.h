@@ -147,6 +147,7 @@ struct GridState {
     long long* partl;       // [2*grid]
     int32_t* own;           // [V] nodes in ownership order (CTA c owns a contiguous run)
     int32_t* owner;         // [V] CTA owning each node
+    int32_t* rd;            // [V] nonzero: some other CTA's halo reads the node
     unsigned* prog;         // [kGridMaxCtas] halo blocks each CTA has completed (neighbour waits)
     unsigned* nbm;          // [kGridMaxCtas * kGridNbWords] bit d of row c: CTA d reads c's nodes
     unsigned long long* okey;   // [V] ownership sort keys (Morton code << 32 | node)

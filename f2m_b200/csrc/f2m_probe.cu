@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(32 * kPcWarps) k_partition_check(int n_cases, 
                                                                     unsigned long long* bad) {
     __shared__ double sv[kPcWarps][2][kPcCap];
     __shared__ uint16_t sp[kPcWarps][2][kPcCap];
+    __shared__ uint8_t spos[kPcWarps][kPcCap];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cs = blockIdx.x * kPcWarps + w;
     if (cs >= n_cases) return;
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(32 * kPcWarps) k_partition_check(int n_cases, 
     if (lane == 0) p0 = qpart_ef_vals(sp[w][0], sv[w][0], size, avg, ef_min);
     __syncwarp();
     p0 = __shfl_sync(0xffffffffu, p0, 0);
-    const int p1 = warp_qpart_ef_vals<kPcCap / 32>(sp[w][1], sv[w][1], size, avg, ef_min, lane);
+    const int p1 = warp_qpart_ef_vals<kPcCap / 32>(sp[w][1], sv[w][1], spos[w], size, avg, ef_min, lane);
     __syncwarp();
     bool diff = p0 != p1;
     for (int e = lane; e < size; e += 32) diff |= sp[w][0][e] != sp[w][1][e];

@@ -214,6 +214,7 @@ void carve_grid(Arena& A, GridState& G, int64_t n, int64_t S) {
     G.partl = A.take<long long>(2 * kGridMaxCtas);
     G.own = A.take<int32_t>(n);
     G.owner = A.take<int32_t>(n);
+    G.rd = A.take<int32_t>(n);
     G.prog = A.take<unsigned>(kGridMaxCtas);
     G.nbm = A.take<unsigned>((int64_t)kGridMaxCtas * kGridNbWords);
     G.okey = A.take<unsigned long long>(n);
