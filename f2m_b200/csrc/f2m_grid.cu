@@ -117,6 +117,23 @@ __device__ __forceinline__ double grad_half(int n, const double* Dp, const uint3
 
 constexpr int kPartCap = 128;  // longest list partitioned in shared memory by a warp
 
+// update_EF's copy of node v's list prefix (n slots in list order) to the
+// slot-indexed arena and, when eD is not null, to the shared-memory cache;
+// restrict pointers let the compiler issue an unrolled group's loads before
+// its stores.
+__device__ __forceinline__ void copy_ef_words(const Slot* __restrict__ ps, double* __restrict__ gD,
+                                              uint32_t* __restrict__ gW, double* __restrict__ eD,
+                                              uint32_t* __restrict__ eW, int n, int v) {
+#pragma unroll 4
+    for (int k = 0; k < n; ++k) {
+        const Slot sl = ps[k];
+        const uint32_t w = (uint32_t)sl.nbr | (sl.nbr < v ? 0x80000000u : 0u);
+        gD[k] = sl.D;
+        gW[k] = w;
+        if (eD) { eD[k] = sl.D; eW[k] = w; }
+    }
+}
+
 // Open-addressing table node -> local index in shared memory (the halo
 // build).  An entry is (node << 32 | local index); node ids are below 2^31,
 // so the all-ones word marks a free entry.
@@ -428,13 +445,7 @@ struct GridSolver {
             const int n = G.efc[v], lo = sefo[i];
             const int64_t go = r0 - row0;
             const bool sm = lo + n <= cap;
-            for (int k = 0; k < n; ++k) {
-                const Slot s = I.pslot[r0 + k];
-                const uint32_t w = (uint32_t)s.nbr | (s.nbr < v ? 0x80000000u : 0u);
-                G.gD[go + k] = s.D;
-                G.gW[go + k] = w;
-                if (sm) { eD[lo + k] = s.D; eW[lo + k] = w; }
-            }
+            copy_ef_words(I.pslot + r0, G.gD + go, G.gW + go, sm ? eD + lo : nullptr, sm ? eW + lo : nullptr, n, v);
         }
         __syncthreads();
         L.built = false;
@@ -578,9 +589,21 @@ struct GridSolver {
                 if (lane == 0) L.sb[sl + 1] = wdt * 32;
             }
             __syncthreads();
-            if (threadIdx.x == 0) {
-                L.sb[0] = 0;
-                for (int sl = 1; sl <= ns; ++sl) L.sb[sl] += L.sb[sl - 1];
+            if (threadIdx.x < 32) {  // prefix of the slice sizes (ns <= 64), one warp
+                const int lane = threadIdx.x;
+                int carry = 0;
+                for (int c0 = 1; c0 <= ns; c0 += 32) {
+                    const int sl = c0 + lane;
+                    int x = sl <= ns ? L.sb[sl] : 0;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (lane >= o) x += y;
+                    }
+                    if (sl <= ns) L.sb[sl] = carry + x;
+                    carry += __shfl_sync(0xffffffffu, x, 31);
+                }
+                if (lane == 0) L.sb[0] = 0;
             }
             __syncthreads();
             for (int k = depth; k >= 1; --k)

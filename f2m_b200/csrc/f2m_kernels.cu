@@ -876,6 +876,30 @@ __device__ __forceinline__ double half_grad(int n, Get get) {
     return (-(v1 + v2) / 2) * 0.5;
 }
 
+// Copies of the active sets (update_EF), with restrict pointers so that the
+// compiler may issue the loads of an unrolled group before its stores.
+// node v's list prefix (n slots in list order) -> its node-indexed copy
+__device__ __forceinline__ void copy_ef_prefix(const Slot* __restrict__ ps, double* __restrict__ gD,
+                                               uint16_t* __restrict__ gN, int n, int v) {
+#pragma unroll 4
+    for (int k = 0; k < n; ++k) {
+        const Slot sl = ps[k];
+        gD[k] = sl.D;
+        gN[k] = (uint16_t)(sl.nbr | (sl.nbr < v ? 0x8000 : 0));
+    }
+}
+// one lane's column of a SELL-32 slice of width wdt from a node-indexed list
+// of n entries (padding: +inf, word 0)
+__device__ __forceinline__ void fill_slice_lane(const double* __restrict__ gD, const uint16_t* __restrict__ gN,
+                                                int n, int wdt, double* __restrict__ dD, uint16_t* __restrict__ dW) {
+#pragma unroll 4
+    for (int k = 0; k < wdt; ++k) {
+        const bool real = k < n;
+        dD[32 * k] = real ? gD[k] : INFINITY;
+        dW[32 * k] = real ? gN[k] : (uint16_t)0;
+    }
+}
+
 template <int TEAM>
 struct Solver {
     static constexpr int WARPS = TEAM / 32;
@@ -964,11 +988,7 @@ struct Solver {
                 const int64_t r0 = I.row[v];
                 const int64_t go = r0 - row0;
                 const int n = M.cnt[v];
-                for (int k = 0; k < n; ++k) {
-                    const Slot s = I.pslot[r0 + k];
-                    I.gD[go + k] = s.D;
-                    I.gN[go + k] = ef_word(v, s.nbr);
-                }
+                copy_ef_prefix(I.pslot + r0, I.gD + go, I.gN + go, n, v);
             }
         }
         // counting sort by list length, longest first (bucket 255 = 255 or more)
@@ -1030,11 +1050,7 @@ struct Solver {
             const int v = (p < V) ? (int)M.ord[p] : -1;
             const int n = (v >= 0) ? M.cnt[v] : 0;
             const int64_t go = (v >= 0) ? I.row[v] - row0 : 0;
-            for (int k = 0; k < M.swid[s]; ++k) {
-                const bool real = k < n;
-                dD[32 * k + lane] = real ? I.gD[go + k] : INFINITY;
-                dW[32 * k + lane] = real ? I.gN[go + k] : (uint16_t)0;
-            }
+            fill_slice_lane(I.gD + go, I.gN + go, n, M.swid[s], dD + lane, dW + lane);
         }
         T.sync();
     }
