@@ -581,17 +581,26 @@ def smooth_sub(args, local_rank, steps=3, warmup=1):
         ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
     clk = Clocks(local_rank)
     l0 = ctx.kernel_launches()
-    ms = []
+    ms, kterms, kms = [], [], []
     clk.start()
     for _ in range(steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         L, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
         ms.append(1e3 * (time.perf_counter() - t0))
+        tr, km = ctx.smooth_work()  # logistic terms and time of the persistent kernel
+        kterms.append(tr)
+        kms.append(km)
     clocks = clk.stop()
     launches = ctx.kernel_launches() - l0
+    # roofline: the persistent kernel (one CTA per instance) evaluates
+    # logistic terms (one FP64 exp and two divisions each: the Newton sums
+    # of every node root, softplus, sigma and sigma'); its peak is the same
+    # term measured at full occupancy on this GPU
+    peak_terms = ctx.fp64_rate(2, repeats=3)
     ctx.close()
     t = float(np.mean(ms))
+    achieved = float(np.mean(kterms)) / (float(np.mean(kms)) / 1e3)
     out = {
         "metric": "smoothed F2M bound + coordinate gradient, instances/s",
         "value": n_inst / (t / 1e3), "unit": "instances/s", "steps": steps, "warmup": warmup,
@@ -604,6 +613,13 @@ def smooth_sub(args, local_rank, steps=3, warmup=1):
                 "d2h_bytes_per_step": int(L.nbytes + gx.nbytes + gy.nbytes)},
         "clocks": clocks, "gpu_launches": int(launches // max(steps, 1)),
         "L_mean": float(np.mean(L)),
+        "roofline": {"bound": "fp64 exp+div", "kernel": "k_sbound (persistent, one CTA per instance)",
+                     "achieved": achieved / 1e9, "peak": peak_terms / 1e9, "unit": "G logistic terms/s",
+                     "frac": achieved / peak_terms if peak_terms > 0 else None,
+                     "peak_kind": "measured in this run (f2m_fp64_rate kind 2: the same term, four "
+                                  "independent sums per thread, every SM at full occupancy)",
+                     "terms_per_launch": float(np.mean(kterms)), "kernel_ms": float(np.mean(kms)),
+                     "traffic": None},
     }
     if not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -728,15 +744,28 @@ def smooth_arm(args, rank, world, local_rank):
         ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
     clk = Clocks(local_rank)
     l0 = ctx.kernel_launches()
-    ms = []
+    ms, kterms, kms = [], [], []
     clk.start()
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         L, gx, gy = ctx.smoothed_bound(offs, x, y, N, params=p, grad=True)
         ms.append(1e3 * (time.perf_counter() - t0))
+        tr, km = ctx.smooth_work()
+        kterms.append(tr)
+        kms.append(km)
     clocks = clk.stop()
     launches = ctx.kernel_launches() - l0
+    roof = None
+    if min(kterms) >= 0 and np.mean(kms) > 0:  # the persistent kernel ran (its terms are counted)
+        peak_terms = ctx.fp64_rate(2, repeats=3)
+        ach = float(np.mean(kterms)) / (float(np.mean(kms)) / 1e3)
+        roof = {"bound": "fp64 exp+div", "kernel": "k_sbound (persistent, one CTA per instance)",
+                "achieved": ach / 1e9, "peak": peak_terms / 1e9, "unit": "G logistic terms/s",
+                "frac": ach / peak_terms if peak_terms > 0 else None,
+                "peak_kind": "measured in this run (f2m_fp64_rate kind 2)",
+                "terms_per_launch": float(np.mean(kterms)), "kernel_ms": float(np.mean(kms)),
+                "traffic": None}
     t = float(np.mean(ms))
     if world > 1:
         tt = torch.tensor([t], dtype=torch.float64, device=torch.device("cuda", local_rank))
@@ -752,7 +781,7 @@ def smooth_arm(args, rank, world, local_rank):
         "config": {"workload": desc, "top_k": N, "tau": p.tau, "iters": p.iters,
                    "damping": p.damping, "checkpoint": p.checkpoint,
                    "parallelism": f"instance sharding over {world} GPU(s), no collective"},
-        "roofline": None,
+        "roofline": roof,
         "e2e": {"value": n_inst * world / (t / 1e3), "unit": "instances/s",
                 "h2d_bytes_per_step": int(offs.nbytes + x.nbytes + y.nbytes),
                 "d2h_bytes_per_step": int(L.nbytes + gx.nbytes + gy.nbytes)},

@@ -92,7 +92,7 @@ EXPORTS = [
     "f2m_solve_points_noalloc", "f2m_default_smooth_params", "f2m_smoothed_bound_fwd",
     "f2m_smoothed_bound_bwd", "f2m_smooth_max_nodes", "f2m_knn", "f2m_set_class_bounds",
     "f2m_get_class_bounds", "f2m_solve_graph", "f2m_solve_points_from", "f2m_fp64_rate",
-    "f2m_partition_selfcheck",
+    "f2m_partition_selfcheck", "f2m_smooth_work",
     "f2m_smoothed_bound_bwd_edges", "f2m_set_solver_smem_kb", "f2m_get_solver_smem_kb",
 ]
 
@@ -137,6 +137,7 @@ def lib():
         L.f2m_phase_times.argtypes = [vp, vp, P(Work)]
         L.f2m_fp64_rate.argtypes = [vp, i32, i32, P(dbl)]
         L.f2m_partition_selfcheck.argtypes = [vp, i32, ctypes.c_uint64, P(ctypes.c_int64)]
+        L.f2m_smooth_work.argtypes = [vp, P(ctypes.c_int64), P(ctypes.c_float)]
         L.f2m_solve_points_noalloc.argtypes = [vp, vp, i32, i32, P(Params), vp, vp, vp]
         L.f2m_default_smooth_params.argtypes = [P(SmoothParams)]
         L.f2m_smoothed_bound_fwd.argtypes = [vp, i32, vp, vp, vp, i32, P(SmoothParams), vp]
@@ -299,10 +300,19 @@ class Context:
 
     def fp64_rate(self, kind=0, repeats=3):
         """Measured FP64 pipe rate of this GPU, FP64 lane operations per second
-        (kind 0: DADD, kind 1: DSETP); the roofline of the dual descent."""
+        (kind 0: DADD, kind 1: DSETP; the roofline of the dual descent), or
+        kind 2: logistic terms per second (the smoothed bound's roofline)."""
         r = ctypes.c_double()
         self._check(lib().f2m_fp64_rate(self._h, kind, repeats, ctypes.byref(r)))
         return r.value
+
+    def smooth_work(self):
+        """(logistic terms, kernel ms) of the last smoothed-bound call's
+        persistent kernel; terms is -1 after the one-launch-per-step path."""
+        t = ctypes.c_int64()
+        ms = ctypes.c_float()
+        self._check(lib().f2m_smooth_work(self._h, ctypes.byref(t), ctypes.byref(ms)))
+        return t.value, ms.value
 
     def partition_selfcheck(self, n_cases=100000, seed=1):
         """Lists on which the warp-cooperative partition and the serial one

@@ -258,6 +258,7 @@ struct SmoothBatch {
     float* gx = nullptr;                // [n_total]
     float* gy = nullptr;                // [n_total]
     int32_t* queue = nullptr;
+    unsigned long long* work = nullptr; // [1] logistic terms evaluated by the persistent kernel
 };
 cudaError_t launch_smooth_graph(SmoothBatch& S, int64_t* scan_scratch, cudaStream_t s,
                                 int64_t* launches);
@@ -265,6 +266,10 @@ cudaError_t launch_smooth_bound(SmoothBatch& S, int32_t max_v, bool grad, cudaSt
                                 int64_t* launches);
 cudaError_t launch_smooth_steps(SmoothBatch& S, bool grad, cudaStream_t s, int64_t* launches);
 int32_t smooth_max_nodes();
+// Rate probe of the smoothed bound's logistic term (one exp and two
+// divisions, the Newton sums' unit of work), and its work per launch.
+cudaError_t launch_logit_probe(int blocks, int iters, double* out, cudaStream_t s);
+double logit_probe_terms(int blocks, int iters);
 
 cudaError_t launch_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* scratch,
                         cudaStream_t s, int64_t* launches);

@@ -76,6 +76,9 @@ struct f2m_ctx {
     cudaGraphExec_t sgraph = nullptr;
     std::vector<int64_t> skey;
     int64_t sgraph_launches = 0;
+    // work and kernel time of the last smoothed-bound call (persistent path)
+    int64_t smooth_terms = -1;
+    float smooth_ms = 0.f;
 };
 
 namespace {
@@ -1309,8 +1312,8 @@ f2m_status f2m_sync(f2m_ctx* ctx) {
 }
 
 f2m_status f2m_fp64_rate(f2m_ctx* ctx, int32_t kind, int32_t repeats, double* lane_ops_per_s) {
-    if (!ctx || !lane_ops_per_s || (kind != 0 && kind != 1) || repeats < 1)
-        return fail(ctx, F2M_ERR_INPUT, "f2m_fp64_rate: kind 0 or 1, repeats >= 1");
+    if (!ctx || !lane_ops_per_s || kind < 0 || kind > 2 || repeats < 1)
+        return fail(ctx, F2M_ERR_INPUT, "f2m_fp64_rate: kind 0, 1 or 2, repeats >= 1");
     F2M_CUDA(cudaSetDevice(ctx->device));
     int per_sm = 0;
     F2M_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxThreadsPerMultiProcessor, ctx->device));
@@ -1321,16 +1324,25 @@ f2m_status f2m_fp64_rate(f2m_ctx* ctx, int32_t kind, int32_t repeats, double* la
     double best = 0.0;
     for (int r = 0; r <= repeats; ++r) {  // the first launch warms up
         F2M_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
-        F2M_CUDA(launch_fp64_probe(kind, blocks, kIters, out, ctx->stream));
+        if (kind == 2) F2M_CUDA(launch_logit_probe(blocks, kIters / 16, out, ctx->stream));
+        else F2M_CUDA(launch_fp64_probe(kind, blocks, kIters, out, ctx->stream));
         F2M_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
         F2M_CUDA(cudaEventSynchronize(ctx->ev[1]));
         ctx->launches++;
         float ms = 0.f;
         F2M_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
-        if (r > 0 && ms > 0.f) best = std::max(best, fp64_probe_ops(kind, blocks, kIters) / (ms * 1e-3));
+        const double ops = kind == 2 ? logit_probe_terms(blocks, kIters / 16) : fp64_probe_ops(kind, blocks, kIters);
+        if (r > 0 && ms > 0.f) best = std::max(best, ops / (ms * 1e-3));
     }
     ctx->timed = false;  // the phase events now hold the probe's times
     *lane_ops_per_s = best;
+    return F2M_OK;
+}
+
+f2m_status f2m_smooth_work(const f2m_ctx* ctx, int64_t* terms, float* kernel_ms) {
+    if (!ctx) return F2M_ERR_INPUT;
+    if (terms) *terms = ctx->smooth_terms;
+    if (kernel_ms) *kernel_ms = ctx->smooth_ms;
     return F2M_OK;
 }
 
@@ -1970,6 +1982,7 @@ f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const 
         B.L = A.take<double>(n_inst);
         dLd = A.take<double>(n_inst);
         B.queue = A.take<int32_t>(1);
+        B.work = A.take<unsigned long long>(1);
         if (steps) {
             B.ua = A.take<double>(n);
             B.ub = A.take<double>(n);
@@ -2013,12 +2026,25 @@ f2m_status smooth_call(f2m_ctx* ctx, int32_t n_inst, const int64_t* offs, const 
     F2M_CUDA(cudaMemcpyAsync(dLd, up.data(), n_inst * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     F2M_CUDA(launch_smooth_graph(B, scan, ctx->stream, &ctx->launches));
     B.solver = steps ? 2 : 1;
-    if (steps) F2M_CUDA(smooth_steps_graph(ctx, B, grad));
-    else F2M_CUDA(launch_smooth_bound(B, max_v, grad, ctx->stream, &ctx->launches));
+    ctx->smooth_terms = -1;
+    ctx->smooth_ms = 0.f;
+    if (steps) {
+        F2M_CUDA(smooth_steps_graph(ctx, B, grad));
+    } else {
+        F2M_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+        F2M_CUDA(launch_smooth_bound(B, max_v, grad, ctx->stream, &ctx->launches));
+        F2M_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+    }
     F2M_CUDA(cudaMemcpyAsync(L, B.L, n_inst * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (gx) F2M_CUDA(cudaMemcpyAsync(gx, B.gx, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     if (gy) F2M_CUDA(cudaMemcpyAsync(gy, B.gy, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    unsigned long long terms = 0;
+    if (!steps) F2M_CUDA(cudaMemcpyAsync(&terms, B.work, sizeof(terms), cudaMemcpyDeviceToHost, ctx->stream));
     F2M_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (!steps) {
+        ctx->smooth_terms = (int64_t)terms;
+        F2M_CUDA(cudaEventElapsedTime(&ctx->smooth_ms, ctx->ev[0], ctx->ev[1]));
+    }
     if (eo && grad) {
         // edges once each (lower point first, in the lower endpoint's list
         // order) with dL/dc_e = the sum of the edge's two slot shares

@@ -217,7 +217,7 @@ __device__ __forceinline__ double root_step(const LogitAcc& r, double tau, doubl
 }
 
 __device__ double node_root(const int32_t* nb, const float* c, int n, const double* u, double tau,
-                            int max_it) {
+                            int max_it, unsigned long long& terms) {
     double m0 = INFINITY, m1 = INFINITY, m2 = INFINITY;
     for (int k = 0; k < n; ++k) top3_insert((double)c[k] - u[nb[k]], m0, m1, m2);
     double lo = m0 - 40 * tau, hi = m2 + 40 * tau;
@@ -225,6 +225,7 @@ __device__ double node_root(const int32_t* nb, const float* c, int n, const doub
     for (int it = 0; it < max_it; ++it) {
         LogitAcc r;
         for (int k = 0; k < n; ++k) r.add((s - ((double)c[k] - u[nb[k]])) / tau);
+        terms += (unsigned long long)n;
         const double sn = root_step(r, tau, s, lo, hi);
         if (sn != sn) break;
         s = sn;
@@ -241,22 +242,23 @@ struct SInst {
 
 // One damped Jacobi step u -> un; writes the roots to s_out when given.
 __device__ __forceinline__ void sjacobi(const SmoothBatch& S, const SInst& I, const double* u,
-                                        double* un, double* s_out) {
+                                        double* un, double* s_out, unsigned long long& terms) {
     for (int v = threadIdx.x; v < I.V; v += kST) {
         const int64_t a = I.row[v], e = I.row[v + 1];
-        const double s = node_root(S.nbr + a, S.c + a, (int)(e - a), u, S.tau, S.newton_max);
+        const double s = node_root(S.nbr + a, S.c + a, (int)(e - a), u, S.tau, S.newton_max, terms);
         if (s_out) s_out[v] = s;
         un[v] = (1.0 - S.omega) * u[v] + S.omega * s;
     }
 }
 
-__device__ double sbound(const SmoothBatch& S, const SInst& I, const double* u, double* sred) {
+__device__ double sbound(const SmoothBatch& S, const SInst& I, const double* u, double* sred,
+                         unsigned long long& terms) {
     double su = 0.0, sp = 0.0;
     for (int v = threadIdx.x; v < I.V; v += kST) {
         su += 2.0 * u[v];
         for (int64_t k = I.row[v]; k < I.row[v + 1]; ++k) {
             const int w = S.nbr[k];
-            if (w > v) sp += softplus((u[v] + u[w] - (double)S.c[k]) / S.tau);
+            if (w > v) { sp += softplus((u[v] + u[w] - (double)S.c[k]) / S.tau); ++terms; }
         }
     }
     su = block_sum<kST>(su, sred);
@@ -270,12 +272,18 @@ __global__ void __launch_bounds__(kST) k_sbound(SmoothBatch S) {
     __shared__ double sred[kST / 32];
     __shared__ int sitem;
     double* Ha = reinterpret_cast<double*>(smem_raw);
+    // logistic terms this thread evaluated (exp-based: Newton sums, softplus,
+    // sigma, sigma'), added to S.work when the queue is empty
+    unsigned long long terms = 0;
     for (;;) {
         if (threadIdx.x == 0) sitem = atomicAdd(S.queue, 1);
         __syncthreads();
         const int b = sitem;
         __syncthreads();
-        if (b >= S.n_inst) return;
+        if (b >= S.n_inst) {
+            if (S.work && terms) atomicAdd(S.work, terms);
+            return;
+        }
         SInst I;
         I.base = S.offs[b];
         I.V = (int)(S.offs[b + 1] - I.base);
@@ -291,11 +299,11 @@ __global__ void __launch_bounds__(kST) k_sbound(SmoothBatch S) {
         for (int t = 0; t < T; ++t) {
             if (GRAD && t % K == 0)
                 for (int v = threadIdx.x; v < I.V; v += kST) ck[(t / K) * I.V + v] = u[v];
-            sjacobi(S, I, u, un, nullptr);
+            sjacobi(S, I, u, un, nullptr, terms);
             __syncthreads();
             double* tt = u; u = un; un = tt;
         }
-        const double L = sbound(S, I, u, sred);
+        const double L = sbound(S, I, u, sred, terms);
         if (threadIdx.x == 0) S.L[b] = L;
         if (!GRAD) { __syncthreads(); continue; }
         // adjoint of L(u^T) with respect to u^T and (explicitly) c; the
@@ -309,6 +317,7 @@ __global__ void __launch_bounds__(kST) k_sbound(SmoothBatch S) {
                 const double z = (u[v] + u[S.nbr[k]] - (double)S.c[k]) / S.tau;
                 r.add(z);
                 S.gc[k] = up * (0.5 * sigm(z));
+                terms += 2;
             }
             lam[v] = up * (-((r.cnt - 2.0) + r.tail));  // 2 - sum sigma
         }
@@ -325,7 +334,7 @@ __global__ void __launch_bounds__(kST) k_sbound(SmoothBatch S) {
             for (int t = t0; t < t1; ++t) {  // recompute the segment's iterates
                 double* ut = su_ + (t - t0) * I.V;
                 for (int v = threadIdx.x; v < I.V; v += kST) ut[v] = u[v];
-                sjacobi(S, I, u, un, ss_ + (t - t0) * I.V);
+                sjacobi(S, I, u, un, ss_ + (t - t0) * I.V, terms);
                 __syncthreads();
                 double* tt = u; u = un; un = tt;
             }
@@ -341,6 +350,7 @@ __global__ void __launch_bounds__(kST) k_sbound(SmoothBatch S) {
                         S.q[k] = p;
                         D += p;
                     }
+                    terms += (unsigned long long)(e - a);
                     const double mu = D > 0 ? S.omega * lam[v] / D : 0.0;  // D == 0: all saturated
                     for (int64_t k = a; k < e; ++k) {
                         const double qk = mu * S.q[k];
@@ -651,6 +661,37 @@ int32_t smooth_max_nodes() {
     return (lim - 1024) / 16;
 }
 
+// Rate of the logistic term at full occupancy: every thread accumulates four
+// independent LogitAcc sums (one exp and two divisions per term, the unit the
+// persistent kernel counts), its arguments moving by a small step each round
+// so that nothing is loop-invariant.
+constexpr int kLogitProbeThreads = 256;
+constexpr int kLogitChains = 4;
+__global__ void __launch_bounds__(kLogitProbeThreads) k_logit_rate(double* out, int iters) {
+    LogitAcc r[kLogitChains];
+    double z[kLogitChains];
+#pragma unroll
+    for (int c = 0; c < kLogitChains; ++c) z[c] = -3.0 + 0.37 * c + 1e-3 * (threadIdx.x & 31);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int c = 0; c < kLogitChains; ++c) {
+            r[c].add(z[c]);
+            z[c] += 1e-4;
+        }
+    }
+    double t = 0.0;
+#pragma unroll
+    for (int c = 0; c < kLogitChains; ++c) t += r[c].cnt + r[c].tail + r[c].scale + r[c].slope;
+    if (t == -1.0) out[blockIdx.x] = t;  // never true: the sums are >= 0; keeps them live
+}
+double logit_probe_terms(int blocks, int iters) {
+    return (double)kLogitChains * (double)iters * (double)blocks * kLogitProbeThreads;
+}
+cudaError_t launch_logit_probe(int blocks, int iters, double* out, cudaStream_t s) {
+    k_logit_rate<<<blocks, kLogitProbeThreads, 0, s>>>(out, iters);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_smooth_bound(SmoothBatch& S, int32_t max_v, bool grad, cudaStream_t s,
                                 int64_t* launches) {
     const size_t dyn = (size_t)max_v * 16;
@@ -665,6 +706,7 @@ cudaError_t launch_smooth_bound(SmoothBatch& S, int32_t max_v, bool grad, cudaSt
     int grid = sms * per_sm;
     if (grid > S.n_inst) grid = S.n_inst;
     if ((e = cudaMemsetAsync(S.queue, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
+    if (S.work && (e = cudaMemsetAsync(S.work, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
     if (grad) k_sbound<true><<<grid, kST, dyn, s>>>(S);
     else k_sbound<false><<<grid, kST, dyn, s>>>(S);
     ++*launches;

@@ -139,8 +139,11 @@ f2m_status f2m_phase_times(f2m_ctx* ctx, float* ms, f2m_work* work);
  * second (diagnostics; no reference counterpart).  The dual descent issues
  * FP64 additions and compares, so this rate, not HBM bandwidth, is the
  * roofline of its persistent solver.  kind 0: independent DADD chains;
- * kind 1: DSETP compares (one DADD per eight).  Best of `repeats` timed
- * launches (CUDA events) over every SM at full occupancy. */
+ * kind 1: DSETP compares (one DADD per eight); kind 2: logistic terms of the
+ * smoothed bound per second (one FP64 exp and two divisions each, four
+ * independent sums per thread), the roofline of its persistent kernel.
+ * Best of `repeats` timed launches (CUDA events) over every SM at full
+ * occupancy. */
 f2m_status f2m_fp64_rate(f2m_ctx* ctx, int32_t kind, int32_t repeats, double* lane_ops_per_s);
 
 /* Self-check of the warp-cooperative list partition (diagnostics; no
@@ -150,6 +153,13 @@ f2m_status f2m_fp64_rate(f2m_ctx* ctx, int32_t kind, int32_t repeats, double* la
  * partition on the device and returns how many differ in order or count
  * (0 when they agree). */
 f2m_status f2m_partition_selfcheck(f2m_ctx* ctx, int32_t n_cases, uint64_t seed, int64_t* mismatches);
+
+/* Work of the last smoothed-bound call on this context (diagnostics; no
+ * reference counterpart): the logistic terms (exp-based evaluations: Newton
+ * sums, softplus, sigma and its derivative) its persistent one-CTA-per-
+ * instance kernel evaluated, and that kernel's CUDA-event time in ms.
+ * terms is -1 when the call took the one-launch-per-step path. */
+f2m_status f2m_smooth_work(const f2m_ctx* ctx, int64_t* terms, float* kernel_ms);
 
 /* ------------------------------------------------------------------ */
 /* Single instance with full results (the F2M.h graph API).             */

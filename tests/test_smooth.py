@@ -140,3 +140,27 @@ def test_per_step_graph_replay_reads_new_inputs(ctx):
         fresh.close()
     assert La[0] != Lb[0]
     assert Lb[0] == Lc[0] and np.array_equal(gb, gc)
+
+
+@pytest.mark.gpu
+def test_work_counter_and_logistic_rate(ctx):
+    """The smoothed bound's roofline counts the logistic terms its persistent
+    kernel evaluates.  Every Jacobi step takes at least one Newton sum per
+    node, each over the node's whole list, so the forward count is at least
+    iters x (list slots); the adjoint adds its recomputed segment and its
+    reverse passes.  The per-step path reports -1 (not counted), and the
+    measured peak of the same term is positive."""
+    import f2m_b200
+    offs, x, y = synth.config5(3, n_inst=16)
+    p = f2m_b200.default_smooth_params(solver=1)
+    ctx.smoothed_bound(offs, x, y, 24, params=p)
+    t_fwd, ms_fwd = ctx.smooth_work()
+    ctx.smoothed_bound(offs, x, y, 24, params=p, grad=True)
+    t_bwd, ms_bwd = ctx.smooth_work()
+    n = int(offs[-1])
+    slots_lb = n * 24  # each point keeps its N nearest: at least N list slots per node
+    assert t_fwd >= p.iters * slots_lb and ms_fwd > 0
+    assert t_bwd > 2 * t_fwd and ms_bwd > ms_fwd
+    ctx.smoothed_bound(offs, x, y, 24, params=f2m_b200.default_smooth_params(solver=2))
+    assert ctx.smooth_work()[0] == -1
+    assert ctx.fp64_rate(2, repeats=1) > 1e9
