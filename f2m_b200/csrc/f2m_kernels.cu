@@ -1068,9 +1068,10 @@ struct Solver {
         checks++;
         return grad_max();
     }
-    // block_EF (graph_cuda.cu:308-338)
-    __device__ void block_ef(int N) {
-        const double MA = grad_max();
+    // block_EF (graph_cuda.cu:308-338).  Every call follows a check_OPT whose
+    // max |grad| was taken over the same potentials and active sets, so that
+    // value is the entry gradient MA.
+    __device__ void block_ef(int N, double MA) {
         int count_M = 0;
         for (int it = 0; it < N; ++it) {
             jacobi();
@@ -1106,7 +1107,7 @@ struct Solver {
         double M_ = check_opt();
         int factor = P.factor0;
         for (int go = 1; go <= P.max_rounds; ++go) {
-            block_ef(factor);
+            block_ef(factor, M_);
             M_ = check_opt();
             if (factor < P.factor_cap) factor += P.factor_step;
             if (M_ < P.error_B) break;
@@ -1118,7 +1119,7 @@ struct Solver {
     __device__ double run_fix() {
         double M_ = check_opt();
         for (int go = 1; go <= P.fix_rounds; ++go) {
-            block_ef(P.fix_factor);
+            block_ef(P.fix_factor, M_);
             M_ = check_opt();
             if (M_ < P.error_B) break;
             if (iters > P.max_iters) { capped = true; break; }
