@@ -443,18 +443,20 @@ class Result:
         self.max_rank = L.f2m_result_max_rank(h)
         self.seconds = L.f2m_result_seconds(h)
         ne, nv = self.n_edges, self.n_nodes
-        self.v1 = np.zeros(ne, np.int32)
-        self.v2 = np.zeros(ne, np.int32)
-        self.lab1 = np.zeros(ne, np.int32)
-        self.lab2 = np.zeros(ne, np.int32)
-        self.Do = np.zeros(ne, np.float64)
-        self.D = np.zeros(ne, np.float64)
-        self.x = np.zeros(ne, np.float64)
+        # every element is written by the library (its host threads fill the
+        # arrays side by side), so no zero fill
+        self.v1 = np.empty(ne, np.int32)
+        self.v2 = np.empty(ne, np.int32)
+        self.lab1 = np.empty(ne, np.int32)
+        self.lab2 = np.empty(ne, np.int32)
+        self.Do = np.empty(ne, np.float64)
+        self.D = np.empty(ne, np.float64)
+        self.x = np.empty(ne, np.float64)
         if ne:
             L.f2m_result_edges(h, *(_ptr(a) for a in (self.v1, self.v2, self.lab1, self.lab2,
                                                       self.Do, self.D, self.x)))
-        self.label = np.zeros(nv, np.int32)
-        self.F = np.zeros(nv, np.float64)
+        self.label = np.empty(nv, np.int32)
+        self.F = np.empty(nv, np.float64)
         if nv:
             L.f2m_result_nodes(h, _ptr(self.label), _ptr(self.F))
         st = Stats()

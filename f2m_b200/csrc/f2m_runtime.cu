@@ -22,6 +22,8 @@
 #include <numeric>
 #include <string>
 #include <unordered_map>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -326,6 +328,31 @@ void carve(Arena& A, Batch& B, const Plan& pl, bool own_inputs, int64_t** deg, i
 /* host comb check and repair loop (the reference's host stage)          */
 /* ------------------------------------------------------------------ */
 // One instance pulled back to the host, in the reference's data model.
+// std::allocator whose value-less construct leaves trivially constructible
+// elements uninitialised: resize() of the large per-edge arrays then skips a
+// serial zero fill of memory that the parallel fills overwrite anyway (every
+// resize of these arrays is followed by a write of every element).
+template <class T>
+struct NoFillAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoFillAlloc<U>;
+    };
+    NoFillAlloc() = default;
+    template <class U>
+    NoFillAlloc(const NoFillAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new ((void*)p) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using hvec = std::vector<T, NoFillAlloc<T>>;
+
 struct HostInst {
     int V = 0, E = 0;
     std::vector<int> label;            // internal id -> TSPLIB label
@@ -335,8 +362,9 @@ struct HostInst {
     std::vector<uint16_t> perm;        // per slot (current list order)
     std::vector<int> mirror;           // per slot
     std::vector<int> slot_edge;        // per slot -> edge id
-    std::vector<int> ev1, ev2, el1, el2, rank1, rank2;  // per edge
-    std::vector<double> eD, eDo;       // per edge
+    hvec<int> ev1, ev2, el1, el2;      // per edge
+    std::vector<int> rank1, rank2;     // per edge
+    hvec<double> eD, eDo;              // per edge
     std::vector<double> F;
     std::vector<int> efcnt, ccnt;
     double dmin = 0;
@@ -746,7 +774,7 @@ struct f2m_result {
     int32_t status = F2M_OK;
     std::string err;
     HostInst H;
-    std::vector<double> x;               // per edge
+    hvec<double> x;                      // per edge
     std::unordered_map<int, double> X;   // graph::X in insertion order
     double lp = NAN;
     int32_t max_rank = 0;
