@@ -297,6 +297,87 @@ __device__ __forceinline__ int qpart_ef_la(const Inst& I, int64_t r0, int v, HP 
     return size;
 }
 
+// The same partition by one thread in the pairing form, for lists of at
+// most 64 entries: one sweep evaluates every position (val(k), kPf at a time,
+// so their loads are in flight together) and marks those > avg; then the
+// Hoare loop's swaps are applied directly -- the t-th marked position below
+// the final count Lc (ascending) with the t-th unmarked one at or above Lc
+// (descending), through swp(i, j) -- and Lc is returned, as qpart_b_la
+// returns it.  *g receives the smallest value > avg (the upper part's
+// minimum the threshold loop needs).  A NaN makes it return -1 before any
+// swap (the caller then runs the plain loop, whose every pass runs).
+template <class Val, class Swap>
+__device__ __forceinline__ int qpart_b_bits(int size, double avg, Val val, Swap swp, double* g) {
+    uint64_t gt = 0;
+    bool nan = false;
+    double gm = INFINITY;
+    for (int k0 = 0; k0 < size; k0 += kPf) {
+        double d[kPf];
+#pragma unroll
+        for (int c = 0; c < kPf; ++c) d[c] = (k0 + c < size) ? val(k0 + c) : 0.0;
+#pragma unroll
+        for (int c = 0; c < kPf; ++c)
+            if (k0 + c < size) {
+                nan |= (d[c] != d[c]);
+                if (d[c] > avg) {
+                    gt |= 1ull << (k0 + c);
+                    gm = fmin(gm, d[c]);
+                }
+            }
+    }
+    if (nan) return -1;
+    *g = gm;
+    if (size <= 1) return size;  // the loop does not run
+    const int Lc = size - __popcll(gt);
+    const uint64_t low = Lc >= 64 ? ~0ull : ((1ull << Lc) - 1ull);
+    const uint64_t all = size >= 64 ? ~0ull : ((1ull << size) - 1ull);
+    uint64_t gL = gt & low, lU = ~gt & all & ~low;
+    while (gL) {
+        const int i = __ffsll((long long)gL) - 1;
+        const int j = 63 - __clzll((long long)lU);
+        gL &= gL - 1ull;
+        lU &= ~(1ull << j);
+        swp(i, j);
+    }
+    return Lc;
+}
+// qpart_ef_vals / qpart_ef_la's threshold loop over qpart_b_bits; returns -1
+// (list untouched) when the list holds a NaN.
+template <class Val, class Swap>
+__device__ __forceinline__ int qpart_ef_bits(int size, double avg, int ef_min, Val val, Swap swp) {
+    if (size < ef_min) return size;
+    constexpr int kLimit = 1 << 20;
+    for (int bump = 0; bump < kLimit;) {
+        double g = INFINITY;
+        const int p = qpart_b_bits(size, avg, val, swp, &g);
+        if (p < 0) return -1;
+        if (p >= ef_min) return p;
+        avg += 1;
+        ++bump;
+        bump_until(avg, bump, g, kLimit);
+    }
+    return size;
+}
+// qpart_ef_la for a node's list in global memory (perm and pslot), by the
+// pairing form when the list has at most 64 entries and no NaN
+template <class HP>
+__device__ __forceinline__ int qpart_ef_pair(const Inst& I, int64_t r0, int v, HP H, int size, double avg,
+                                             int ef_min) {
+    if (size <= 64) {
+        const double hv = H[v];
+        uint16_t* list = I.perm + r0;
+        Slot* ps = I.pslot + r0;
+        const int p = qpart_ef_bits(
+            size, avg, ef_min, [&](int k) { return red_d(ps[k], v, H, hv); },
+            [&](int i, int j) {
+                const uint16_t t = list[i]; list[i] = list[j]; list[j] = t;
+                const Slot u = ps[i]; ps[i] = ps[j]; ps[j] = u;
+            });
+        if (p >= 0) return p;
+    }
+    return qpart_ef_la(I, r0, v, H, size, avg, ef_min);
+}
+
 // qpart_ptr_EF on a node's list copied to shared memory: `pl` holds the list
 // order and `val` the reduced cost of each position.  The loop is qpart_ef's
 // (the Hoare scans, the swaps, which move both arrays, and the threshold

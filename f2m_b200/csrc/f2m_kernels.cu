@@ -1062,7 +1062,7 @@ struct Solver {
     __device__ double check_opt() {
         for (int v = T.tid; v < I.V; v += TEAM) {
             const int d = deg(v);
-            M.cnt[v] = (d < P.ef_small_deg) ? d : qpart_ef_la(I, I.row[v], v, Hc, d, P.ef_thr, P.ef_min);
+            M.cnt[v] = (d < P.ef_small_deg) ? d : qpart_ef_pair(I, I.row[v], v, Hc, d, P.ef_thr, P.ef_min);
         }
         finish_partition();
         checks++;
@@ -1095,7 +1095,7 @@ struct Solver {
                 const double hv = Hc[v];
                 double avg = pdv(I, r0, 0, v, Hc, hv);
                 for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, k, v, Hc, hv));
-                M.cnt[v] = qpart_ef_la(I, r0, v, Hc, d, avg, P.ef_min);
+                M.cnt[v] = qpart_ef_pair(I, r0, v, Hc, d, avg, P.ef_min);
             }
             finish_partition();
             if (grad_max() < P.glob_tol) break;

@@ -81,8 +81,8 @@ constexpr int kPcWarps = 8;
 constexpr int kPcCap = 128;
 __global__ void __launch_bounds__(32 * kPcWarps) k_partition_check(int n_cases, unsigned long long seed,
                                                                     unsigned long long* bad) {
-    __shared__ double sv[kPcWarps][2][kPcCap];
-    __shared__ uint16_t sp[kPcWarps][2][kPcCap];
+    __shared__ double sv[kPcWarps][3][kPcCap];
+    __shared__ uint16_t sp[kPcWarps][3][kPcCap];
     __shared__ uint8_t spos[kPcWarps][kPcCap];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cs = blockIdx.x * kPcWarps + w;
@@ -97,8 +97,8 @@ __global__ void __launch_bounds__(32 * kPcWarps) k_partition_check(int n_cases, 
         double x = (kind == 0) ? (double)(r >> 11) * 0x1.0p-53 * 4.0 - 1.0
                                : (double)(r % (unsigned long long)levels) * 0.5 - 2.0;
         if (nan && e == (int)((h >> 40) % (unsigned long long)(size > 0 ? size : 1))) x = NAN;
-        sv[w][0][e] = sv[w][1][e] = x;
-        sp[w][0][e] = sp[w][1][e] = (uint16_t)e;
+        sv[w][0][e] = sv[w][1][e] = sv[w][2][e] = x;
+        sp[w][0][e] = sp[w][1][e] = sp[w][2][e] = (uint16_t)e;
     }
     __syncwarp();
     const double avg = (kind == 1) ? -3.0 - (double)((h >> 48) % 7) : (double)((int)((h >> 48) % 9) - 4) * 0.25;
@@ -109,8 +109,24 @@ __global__ void __launch_bounds__(32 * kPcWarps) k_partition_check(int n_cases, 
     p0 = __shfl_sync(0xffffffffu, p0, 0);
     const int p1 = warp_qpart_ef_vals<kPcCap / 32>(sp[w][1], sv[w][1], spos[w], size, avg, ef_min, lane);
     __syncwarp();
-    bool diff = p0 != p1;
-    for (int e = lane; e < size; e += 32) diff |= sp[w][0][e] != sp[w][1][e];
+    // the thread-serial pairing form (lists of at most 64 entries without NaN)
+    int p2 = p0;
+    bool pair = size <= 64;
+    if (lane == 0 && pair) {
+        double* val = sv[w][2];
+        uint16_t* pl = sp[w][2];
+        p2 = qpart_ef_bits(
+            size, avg, ef_min, [&](int k) { return val[k]; },
+            [&](int i, int j) {
+                const uint16_t t = pl[i]; pl[i] = pl[j]; pl[j] = t;
+                const double u = val[i]; val[i] = val[j]; val[j] = u;
+            });
+    }
+    __syncwarp();
+    p2 = __shfl_sync(0xffffffffu, p2, 0);
+    pair = pair && p2 >= 0;  // -1: a NaN, which the pairing form leaves to the serial loop
+    bool diff = p0 != p1 || (pair && p2 != p0);
+    for (int e = lane; e < size; e += 32) diff |= sp[w][0][e] != sp[w][1][e] || (pair && sp[w][0][e] != sp[w][2][e]);
     if (__any_sync(0xffffffffu, diff) && lane == 0) atomicAdd(bad, 1ull);
 }
 
