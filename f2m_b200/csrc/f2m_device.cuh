@@ -173,9 +173,17 @@ __device__ __forceinline__ double pdv(const Inst& I, int64_t r0, int k, int v, H
 }
 // Sets pslot from slot and perm for nodes [v0, V) in steps of `step` (each
 // solver keeps the two in step from there: every swap moves both).
+// (restrict pointers: an unrolled group's loads may be issued before its stores)
+__device__ __forceinline__ void gather_slots(const Slot* __restrict__ slot, const uint16_t* __restrict__ perm,
+                                             Slot* __restrict__ out, int64_t n) {
+#pragma unroll 4
+    for (int64_t k = 0; k < n; ++k) out[k] = slot[perm[k]];
+}
 __device__ __forceinline__ void init_pslot(const Inst& I, int v0, int step) {
-    for (int v = v0; v < I.V; v += step)
-        for (int64_t a = I.row[v]; a < I.row[v + 1]; ++a) I.pslot[a] = I.slot[I.row[v] + I.perm[a]];
+    for (int v = v0; v < I.V; v += step) {
+        const int64_t r0 = I.row[v];
+        gather_slots(I.slot + r0, I.perm + r0, I.pslot + r0, I.row[v + 1] - r0);
+    }
 }
 
 // The threshold loop of qpart_ptr_EF, `while (avg < g && bump < limit) {
@@ -357,6 +365,26 @@ __device__ __forceinline__ int qpart_ef_bits(int size, double avg, int ef_min, V
         bump_until(avg, bump, g, kLimit);
     }
     return size;
+}
+// qpart_b_la (one pass) for a node's list in global memory, by the pairing
+// form when the list has at most 64 entries and no NaN
+template <class HP>
+__device__ __forceinline__ int qpart_b_pair(const Inst& I, int64_t r0, int v, HP H, int size, double avg) {
+    if (size <= 64) {
+        const double hv = H[v];
+        uint16_t* list = I.perm + r0;
+        Slot* ps = I.pslot + r0;
+        double g;
+        const int p = qpart_b_bits(
+            size, avg, [&](int k) { return red_d(ps[k], v, H, hv); },
+            [&](int i, int j) {
+                const uint16_t t = list[i]; list[i] = list[j]; list[j] = t;
+                const Slot u = ps[i]; ps[i] = ps[j]; ps[j] = u;
+            },
+            &g);
+        if (p >= 0) return p;
+    }
+    return qpart_b_la(I, r0, v, H, size, avg);
 }
 // qpart_ef_la for a node's list in global memory (perm and pslot), by the
 // pairing form when the list has at most 64 entries and no NaN

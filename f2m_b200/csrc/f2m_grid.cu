@@ -764,7 +764,7 @@ struct GridSolver {
                     avg = pdv(I, r0, 0, v, H, hv);
                     for (int k = 1; k < P.glob_K; ++k) avg = fmax(avg, pdv(I, r0, k, v, H, hv));
                 }
-                G.efc[v] = qpart_ef_la(I, r0, v, H, d, avg, P.ef_min);
+                G.efc[v] = qpart_ef_pair(I, r0, v, H, d, avg, P.ef_min);
             }
             __syncthreads();
             return;
@@ -880,7 +880,7 @@ struct GridSolver {
         int* lab = G.scratch + V;
         for (int i = threadIdx.x; i < nown(); i += kGT) {  // cuda_partition_v3
             const int v = node(i);
-            ccnt[v] = qpart_b_la(I, I.row[v], v, hc(), G.efc[v], P.comb_thr);
+            ccnt[v] = qpart_b_pair(I, I.row[v], v, hc(), G.efc[v], P.comb_thr);
         }
         for (int i = threadIdx.x; i < nown(); i += kGT) {
             const int v = node(i);
@@ -1106,7 +1106,8 @@ __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, Gri
     // the own nodes' slots in list order (the host paths upload slot and perm)
     for (int i = threadIdx.x; i < nv; i += kGT) {
         const int v = S.node(i);
-        for (int64_t a = I.row[v]; a < I.row[v + 1]; ++a) I.pslot[a] = I.slot[I.row[v] + I.perm[a]];
+        const int64_t r0 = I.row[v];
+        gather_slots(I.slot + r0, I.perm + r0, I.pslot + r0, I.row[v + 1] - r0);
     }
     if (!refit) {
         for (int i = threadIdx.x; i < nv; i += kGT) {

@@ -995,16 +995,39 @@ struct Solver {
         for (int k = T.tid; k < 257; k += TEAM) M.hist[k] = 0;
         tot = T.sum_ll(tot);  // (also orders the hist reset before its use)
         if (T.tid == 0) M.hist[256] = (int)tot;
-        for (int v = T.tid; v < V; v += TEAM) atomicAdd(&M.hist[255 - min(M.cnt[v], 255)], 1);
-        T.sync();
-        if (T.tid == 0) {
-            int run = 0;
-            for (int k = 0; k < 256; ++k) { const int c = M.hist[k]; M.hist[k] = run; run += c; }
+        // (lanes with the same bucket add once per warp: few buckets, many nodes)
+        for (int v0 = T.tid & ~31; v0 < V; v0 += TEAM) {
+            const int v = v0 + (T.tid & 31);
+            const int key = v < V ? 255 - min(M.cnt[v], 255) : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            if (key >= 0 && (T.tid & 31) == __ffs(peers) - 1) atomicAdd(&M.hist[key], __popc(peers));
         }
         T.sync();
-        for (int v = T.tid; v < V; v += TEAM) {
-            const int p = atomicAdd(&M.hist[255 - min(M.cnt[v], 255)], 1);
-            M.ord[p] = (uint16_t)v;
+        if (T.tid < 32) {  // exclusive scan of the 256 buckets, 8 per lane
+            const int l = T.tid;
+            int c[8], run = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) { c[j] = M.hist[8 * l + j]; run += c[j]; }
+            int inc = run;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (l >= o) inc += y;
+            }
+            int base = inc - run;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) { M.hist[8 * l + j] = base; base += c[j]; }
+        }
+        T.sync();
+        for (int v0 = T.tid & ~31; v0 < V; v0 += TEAM) {
+            const int lane_ = T.tid & 31, v = v0 + lane_;
+            const int key = v < V ? 255 - min(M.cnt[v], 255) : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            const int leader = __ffs(peers) - 1;
+            int base = 0;
+            if (key >= 0 && lane_ == leader) base = atomicAdd(&M.hist[key], __popc(peers));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (key >= 0) M.ord[base + __popc(peers & ((1u << lane_) - 1u))] = (uint16_t)v;
         }
         T.sync();
         // slice widths (longest list of the slice) and offsets in the cache
@@ -1134,7 +1157,7 @@ struct Solver {
         int* ccnt = reinterpret_cast<int*>(Hn);  // Hn is free: room for 2V ints
         int* lab = ccnt + V;
         for (int v = T.tid; v < V; v += TEAM)  // cuda_partition_v3
-            ccnt[v] = qpart_b_la(I, I.row[v], v, Hc, M.cnt[v], P.comb_thr);
+            ccnt[v] = qpart_b_pair(I, I.row[v], v, Hc, M.cnt[v], P.comb_thr);
         T.sync();
         for (int v = T.tid; v < V; v += TEAM) {
             const int64_t r0 = I.row[v];
