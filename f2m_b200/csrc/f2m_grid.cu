@@ -736,7 +736,7 @@ struct GridSolver {
 
     // update_EF's partitions of the own nodes' lists (cuda_partition_v2 with
     // threshold thr, or v4 with the largest of the first glob_K reduced costs
-    // when glob): warp w takes the own nodes w, w+32, ...; a list of up to
+    // when glob): warps take the own nodes from a shared counter; a list of up to
     // kPartCap entries is copied with its reduced costs into the warp's
     // shared scratch in one parallel round of loads and partitioned there by
     // the whole warp (warp_qpart_ef_vals; the halo region is free here: it is
@@ -769,7 +769,16 @@ struct GridSolver {
             __syncthreads();
             return;
         }
-        for (int i = wid; i < nown(); i += kGT / 32) {
+        // warps take the own nodes from a shared counter (the halo build's,
+        // free until the next build), so a warp that drew long lists does
+        // not hold up the CTA
+        if (threadIdx.x == 0) L.cnt[0] = 0;
+        __syncthreads();
+        for (;;) {
+            int i = 0;
+            if (lane == 0) i = atomicAdd(L.cnt, 1);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= nown()) break;
             const int v = node(i);
             const int d = deg(v);
             if (glob ? d < P.glob_K : d < P.ef_small_deg) {
