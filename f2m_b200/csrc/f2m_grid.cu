@@ -111,6 +111,8 @@ __device__ __forceinline__ double grad_half(int n, const double* Dp, const uint3
 }
 
 constexpr int kPartCap = 128;  // longest list partitioned in shared memory by a warp
+// halo entries (12 B each) whose room holds the partition scratch of 32 warps
+constexpr int kPartScratchEntries = (32 * kPartCap * 11 + 11) / 12;
 
 // update_EF's copy of node v's list prefix (n slots in list order) to the
 // slot-indexed arena and, when eD is not null, to the shared-memory cache;
@@ -746,7 +748,7 @@ struct GridSolver {
     __device__ void partition_own(bool glob, double thr) {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
         // per warp: kPartCap values (8 B), list entries (2 B) and rank positions (1 B)
-        const bool scratch = L.nl > 0 && (long long)L.ne * 12 >= 32LL * kPartCap * 11;
+        const bool scratch = L.nl > 0 && L.ne >= kPartScratchEntries;
         double* val = L.D + wid * kPartCap;
         uint16_t* pl = reinterpret_cast<uint16_t*>(L.D + 32 * kPartCap) + wid * kPartCap;
         uint8_t* pos = reinterpret_cast<uint8_t*>(reinterpret_cast<uint16_t*>(L.D + 32 * kPartCap) + 32 * kPartCap) +
@@ -1153,20 +1155,38 @@ __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, Gri
 // at 24 B, the rest of the opt-in limit as 12-B entries).  nl is the power of
 // two >= 3x the own nodes, 1,024-2,048; CTAs with more than 2,048 own nodes
 // get no halo and step with one barrier per step.
+// Kilobytes of the SM's shared-memory carve-out left to L1 (F2M_GRID_L1_KB
+// overrides): this 64-register kernel spills, and its local loads miss an L1
+// squeezed by a full shared-memory allocation.  The halo needs far fewer
+// entries than a full allocation gives it on 10^5-point instances (100k
+// points: 0 / 32 / 64 / 80 KB gave 39.8 / 35.9 / 35.2 / 39.4 ms; at 80 KB
+// the halo entries no longer fit the partition scratch).
+static int grid_l1_reserve_kb() {
+    static int kb = -1;
+    if (kb < 0) {
+        const char* e = getenv("F2M_GRID_L1_KB");
+        kb = e ? atoi(e) : 64;
+        if (kb < 0) kb = 0;
+        if (kb > 160) kb = 160;
+    }
+    return kb;
+}
+
 static size_t grid_smem_bytes(int32_t V, int grid, int* cap, int* nl, int* ne) {
     const int nv = (V + grid - 1) / grid + 1;
     size_t off = (((size_t)nv + 1) * 4 + 15) / 16 * 16;
     int dev = 0, lim = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const long long room = (long long)lim - 8192;  // static shared memory and alignment
+    // static shared memory and alignment, and the L1 reserve
+    const long long room = (long long)lim - 8192 - 1024LL * grid_l1_reserve_kb();
     int l = 1024;
     while (l < 3 * nv && l < kMaxNl) l *= 2;
     if (nv > kMaxNl) l = 0;
     long long c = l ? (long long)nv * 3 : (room - (long long)off) / 12;
     const long long halo_nodes = l ? (long long)l * 24 + 16 : 0;
     long long e = l ? (room - (long long)off - c * 12 - 16 - halo_nodes) / 12 : 0;
-    if (l && e < 4LL * l) {  // not enough room for a useful halo
+    if (l && e < std::max(2LL * l, (long long)kPartScratchEntries)) {  // not enough room for a useful halo
         l = 0;
         e = 0;
         c = (room - (long long)off) / 12;
