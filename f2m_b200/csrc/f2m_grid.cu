@@ -1159,8 +1159,9 @@ __global__ void __launch_bounds__(kGT, 1) k_solve_grid(Batch B, DevParams P, Gri
 // overrides): this 64-register kernel spills, and its local loads miss an L1
 // squeezed by a full shared-memory allocation.  The halo needs far fewer
 // entries than a full allocation gives it on 10^5-point instances (100k
-// points: 0 / 32 / 64 / 80 KB gave 39.8 / 35.9 / 35.2 / 39.4 ms; at 80 KB
-// the halo entries no longer fit the partition scratch).
+// points: 0 / 32 / 48 / 56 / 64 / 72 / 80 KB gave 39.8 / 35.9 / 35.9 / 35.9 /
+// 34.9-35.2 / 38.5 / 39.4 ms: past 64 KB the halo of the long phases stops
+// fitting).
 static int grid_l1_reserve_kb() {
     static int kb = -1;
     if (kb < 0) {
