@@ -419,6 +419,34 @@ def test_grid_block_depths_give_identical_potentials(tmp_path):
         assert _close(float(out[k]["lp"]), float(out[0]["lp"]))
 
 
+def test_grid_l1_reserve_gives_identical_potentials(tmp_path):
+    """The whole-GPU solver leaves part of the shared-memory carve-out to L1
+    (F2M_GRID_L1_KB), which changes how many halo entries fit and so the
+    block depth of each phase and whether the partitions run in shared
+    memory -- never the potentials, the primal or the iteration count (at
+    160 KB the halo no longer fits and every step meets a grid barrier).
+    The reserve is read once per process, so each setting runs in a child
+    process."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import f2m_b200; from f2m_b200 import synth; "
+            "x, y = synth.config2(5, n=20000); r = f2m_b200.Context(0).solve_points(x, y, 16, "
+            "params=f2m_b200.default_params(solver=2)); np.savez(sys.argv[1], F=r.F, x=r.x, lp=r.lp, "
+            "it=r.stats['iterations'])" % root)
+    out = {}
+    for kb in (0, 64, 160):
+        f = str(tmp_path / f"kb{kb}.npz")
+        env = dict(os.environ, F2M_GRID_L1_KB=str(kb))
+        subprocess.run([sys.executable, "-c", code, f], env=env, check=True, timeout=600)
+        out[kb] = np.load(f)
+    for kb in (64, 160):
+        assert np.array_equal(out[kb]["F"], out[0]["F"]), f"L1 reserve {kb} KB changed the potentials"
+        assert np.array_equal(out[kb]["x"], out[0]["x"])
+        assert int(out[kb]["it"]) == int(out[0]["it"])
+        assert _close(float(out[kb]["lp"]), float(out[0]["lp"]))
+
+
 def test_repeated_calls_are_bit_identical(ctx):
     """Replays: every reduction here has a fixed order (team sums, the grid
     solver's per-CTA partials read in CTA order), so the same call gives the
